@@ -1,0 +1,458 @@
+#!/usr/bin/env python
+"""Benchmark of the batched multi-query traversal path.
+
+Workload (one step): a batch of 256 BFS queries and a batch of 256 SSSP
+queries over an R-MAT scale-22 graph (edge factor 16, a=.57 b=.19 c=.19,
+symmetrised, deduplicated, self loops removed, int32 CSR, uint32 weights
+uniform in [1,64]); sources drawn with a fixed seed from the largest
+component; 4 x 64-bit query-mask words per vertex.  Output: int32 depths and
+uint32 distances per (vertex, query), written to device buffers.
+
+Metric: aggregate GTEPS = sum over queries of the directed CSR entries of the
+vertices each query reached, divided by the step time (init included).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank runs its own 256+256 queries on its own GPU
+(queries are independent: no collective on the data path; weak scaling); the
+time is the max over ranks.  `--impl reference` times the reference's own
+CPU traversal (compiled from the reference sources into oracle/_ref) on the
+host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L2_BYTES = 126 * 2**20
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="cgp", choices=["cgp", "reference"])
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--edge-factor", type=int, default=16)
+    p.add_argument("--nbfs", type=int, default=256)
+    p.add_argument("--nsssp", type=int, default=256)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-one-query", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--mode", default="hybrid")
+    p.add_argument("--json-out", default="")
+    return p.parse_args()
+
+
+# ------------------------------------------------------------------ workload
+def make_graph(args):
+    import cgp_b200 as cgp
+    t = time.perf_counter()
+    g = cgp.gen_rmat(args.scale, args.edge_factor, 0.57, 0.19, 0.19, seed=1)
+    g = g.with_weights("u32", 1, 64, seed=2)
+    return g, time.perf_counter() - t
+
+
+def largest_component(g, labels):
+    deg = g.degrees()
+    lab = labels.astype(np.int64)
+    counts = np.bincount(lab, minlength=g.num_vertices)
+    big = int(np.argmax(counts))
+    allowed = (lab == big)
+    comp_edges = int(deg[allowed].sum())
+    return allowed, comp_edges, int(allowed.sum())
+
+
+def workload_name(args):
+    return f"rmat{args.scale}_ef{args.edge_factor}_bfs{args.nbfs}_sssp{args.nsssp}"
+
+
+def sample_sources(g, allowed, args, rank):
+    n = args.nbfs + args.nsssp
+    src = g.pick_sources(n, seed=42 + 1000 * rank, allowed=allowed.astype(np.uint8))
+    return src[:args.nbfs], src[args.nbfs:]
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        sm, mx, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        busy = [s for s, p in zip(sm, power) if p > 0.5 * max(power)] if power else []
+        return {"sm_mhz": statistics.median(busy or sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ----------------------------------------------------------------- roofline
+def level_bytes(profiles, kind, V, W, ob=4):
+    """Algorithmic bytes per kernel class from the per-level counters.
+    BFS push: U(2o+Wb+4) + D(4+2Wb) + 4N + Wb U'
+    BFS pull: 2 V Wb + P 2o + S(4+Wb) + 4N
+    SSSP push: U(2o+Wb+4) + D(4+4+Wb) + 4 sum(popc) + 8 A + Wb U'"""
+    Wb = 8 * W
+    out = {"bfs_push": 0, "bfs_pull": 0, "sssp_push": 0}
+    for p in profiles:
+        U, D, N, Un = p.frontier_size, p.frontier_edges, p.new_pairs, p.next_size
+        if kind == "bfs":
+            if p.mode == "push":
+                out["bfs_push"] += U * (2 * ob + Wb + 4) + D * (4 + 2 * Wb) + 4 * N + Wb * Un
+            else:
+                out["bfs_pull"] += (2 * V * Wb + p.pull_vertices * 2 * ob
+                                    + p.pull_edges * (4 + Wb) + 4 * N)
+        else:
+            out["sssp_push"] += (U * (2 * ob + Wb + 4) + D * (4 + 4 + Wb) + 4 * p.sssp_active
+                                 + 8 * p.sssp_pairs + Wb * Un)
+    return out
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# -------------------------------------------------------------- CPU sides
+def cpu_reference_sample(g, bfs_src, sssp_src, threads):
+    """The reference's cpu_bfs / cpu_sssp (oracle/_ref) when compiled here,
+    else the C restatement, over `threads` host threads.  Returns
+    (seconds, edges, kind, outputs)."""
+    import oracle
+    gf = type(g)(g.row_offsets, g.col_indices, g.weights.astype(np.float32))
+    t = time.perf_counter()
+    if oracle.has_ref():
+        kind = "reference"
+        b = oracle.ref_batch("bfs", gf, bfs_src, threads=threads)
+        s = oracle.ref_batch("sssp", gf, sssp_src, threads=threads)
+    else:
+        kind = "port"
+        b, _ = oracle.batch("bfs", g, bfs_src, threads=threads)
+        s, _ = oracle.batch("sssp", g, sssp_src, threads=threads)
+    dt = time.perf_counter() - t
+    deg = g.degrees()
+    edges = int(sum(deg[row != 2**31 - 1].sum() for row in b))
+    edges += int(sum(deg[np.isfinite(row)].sum() for row in s)) if s.dtype == np.float32 else \
+        int(sum(deg[row != 2**32 - 1].sum() for row in s))
+    return dt, edges, kind, (b, s)
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import cgp_b200 as cgp  # generators only (host code)
+    import oracle
+    g, _ = make_graph(args)
+    labels = oracle.wcc_components(g)
+    allowed, comp_edges, comp_v = largest_component(g, labels)
+    bfs_src, sssp_src = sample_sources(g, allowed, args, 0)
+    threads = os.cpu_count() or 1
+    nb = min(len(bfs_src), max(1, threads))
+    ns = min(len(sssp_src), max(1, threads // 2))
+    for _ in range(args.warmup):
+        cpu_reference_sample(g, bfs_src[:min(nb, 2)], sssp_src[:1], threads)
+    times, edges = [], 0
+    kind = "port"
+    for _ in range(args.steps):
+        dt, e, kind, _ = cpu_reference_sample(g, bfs_src[:nb], sssp_src[:ns], threads)
+        times.append(dt)
+        edges = e
+    t = sum(times)
+    value = args.steps * edges / t / 1e9
+    sample = (f"{nb} BFS + {ns} SSSP queries of the {workload_name(args)} workload per step "
+              f"(of {args.nbfs}+{args.nsssp}), reference cpu_bfs/cpu_sssp, one query per thread")
+    line = {
+        "impl": "reference", "metric": "aggregate GTEPS", "value": value, "unit": "GTEPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": workload_name(args), "scale": args.scale,
+                   "edge_factor": args.edge_factor, "V": g.num_vertices, "E": g.num_edges},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    import torch
+    import torch.distributed as dist
+    import cgp_b200 as cgp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and world > 1:
+        print(f"warning: WORLD_SIZE={world} but --gpus={args.gpus}", file=sys.stderr)
+    torch.cuda.set_device(local)
+    cgp.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allreduce(x, op):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=op)
+        return t.item()
+
+    g, gen_s = make_graph(args)
+    graph = cgp.CsrGraph(g, symmetric=True)
+    labels = cgp.run("wcc", graph, [0]).values[:, 0]
+    allowed, comp_edges, comp_v = largest_component(g, labels)
+    bfs_src, sssp_src = sample_sources(g, allowed, args, rank)
+    V = g.num_vertices
+    bfs_d = [cgp.QueryDescriptor(int(s), "bfs") for s in bfs_src]
+    sssp_d = [cgp.QueryDescriptor(int(s), "sssp") for s in sssp_src]
+    out_b = torch.empty((V, len(bfs_d)), dtype=torch.int32, device=dev)
+    out_s = torch.empty((V, len(sssp_d)), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    opts = cgp.RunOptions(traversal_mode=args.mode, stream=stream.cuda_stream)
+
+    def step():
+        rb = cgp.run_batch(graph, bfs_d, opts, out=out_b)
+        rs = cgp.run_batch(graph, sssp_d, opts, out=out_s)
+        return rb, rs
+
+    for _ in range(max(3, args.warmup)):
+        rb, rs = step()
+    # every query reaches exactly the largest component (symmetric graph)
+    reached_b = int((out_b != 2**31 - 1).sum().item())
+    reached_s = int((out_s != -1).sum().item())
+    assert reached_b == comp_v * len(bfs_d), (reached_b, comp_v)
+    assert reached_s == comp_v * len(sssp_d), (reached_s, comp_v)
+    edges_step = comp_edges * (len(bfs_d) + len(sssp_d))
+
+    launches = 0
+    t_b = t_s = 0.0
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rb, rs = step()
+            launches += rb.kernel_launches + rs.kernel_launches
+            t_b += rb.gpu_time_ms
+            t_s += rs.gpu_time_ms
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = allreduce(ms, dist.ReduceOp.MAX if world > 1 else None)
+    total_edges = allreduce(edges_step * args.steps, dist.ReduceOp.SUM if world > 1 else None)
+    value = total_edges / (ms_max / 1e3) / 1e9
+    qps = (len(bfs_d) + len(sssp_d)) * args.steps * world / (ms_max / 1e3)
+
+    # ---- profiled step: per-kernel-class CUDA-event times + level counters
+    popts = cgp.RunOptions(traversal_mode=args.mode, stream=stream.cuda_stream,
+                           profile_kernels=True, profile_iterations=True)
+    pb = cgp.run_batch(graph, bfs_d, popts, out=out_b)
+    ps = cgp.run_batch(graph, sssp_d, popts, out=out_s)
+    W = pb.mask_words
+    bytes_b = level_bytes(pb.iteration_profiles, "bfs", V, W)
+    bytes_s = level_bytes(ps.iteration_profiles, "sssp", V, ps.mask_words)
+    kclass = {}
+    for name in ("bfs_push", "bfs_pull"):
+        if name in pb.kernel_profile:
+            ms_k, n_k = pb.kernel_profile[name]
+            kclass[name] = {"ms": ms_k, "launches": n_k, "bytes": bytes_b[name]}
+    if "sssp_push" in ps.kernel_profile:
+        ms_k, n_k = ps.kernel_profile["sssp_push"]
+        kclass["sssp_push"] = {"ms": ms_k, "launches": n_k, "bytes": bytes_s["sssp_push"]}
+    peak, peak_src = measured_peaks()
+    dom = max(kclass, key=lambda k: kclass[k]["ms"]) if kclass else None
+    roofline = None
+    if dom:
+        k = kclass[dom]
+        achieved = k["bytes"] / (k["ms"] / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                    "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+                    "traffic": None, "bytes_per_launch": k["bytes"] / max(1, k["launches"]),
+                    "ms_per_launch": k["ms"] / max(1, k["launches"]),
+                    "classes": {n: {"ms": v["ms"], "launches": v["launches"],
+                                    "GBps": v["bytes"] / max(v["ms"], 1e-9) / 1e6}
+                                for n, v in kclass.items()}}
+
+    # ---- one-query form: the same kernels with Q = 1, back to back
+    one_query = None
+    if not args.no_one_query and rank == 0:
+        nb1, ns1 = min(16, len(bfs_d)), min(8, len(sssp_d))
+        o1 = torch.empty((V, 1), dtype=torch.int32, device=dev)
+        for d in (bfs_d[0], sssp_d[0]):
+            cgp.run_batch(graph, [d], opts, out=o1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for d in bfs_d[:nb1]:
+            cgp.run_batch(graph, [d], opts, out=o1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tb1 = e0.elapsed_time(e1) / nb1
+        e0.record(stream)
+        for d in sssp_d[:ns1]:
+            cgp.run_batch(graph, [d], opts, out=o1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts1 = e0.elapsed_time(e1) / ns1
+        t_one = tb1 * len(bfs_d) + ts1 * len(sssp_d)
+        one_query = {"gteps": edges_step / (t_one / 1e3) / 1e9, "bfs_ms_per_query": tb1,
+                     "sssp_ms_per_query": ts1,
+                     "sample": f"{nb1} BFS + {ns1} SSSP single-query runs, scaled to the batch"}
+
+    # ---- e2e: the public API with host buffers (pinned), copies inside
+    e2e = None
+    if args.e2e_steps > 0:
+        hb = torch.empty((V, len(bfs_d)), dtype=torch.int32, pin_memory=True)
+        hs = torch.empty((V, len(sssp_d)), dtype=torch.int32, pin_memory=True)
+        eopts = cgp.RunOptions(traversal_mode=args.mode)
+        cgp.run_batch(graph, bfs_d, eopts, out=hb)
+        cgp.run_batch(graph, sssp_d, eopts, out=hs)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            cgp.run_batch(graph, bfs_d, eopts, out=hb)
+            cgp.run_batch(graph, sssp_d, eopts, out=hs)
+        t_e2e = time.perf_counter() - t0
+        t_e2e = allreduce(t_e2e, dist.ReduceOp.MAX if world > 1 else None)
+        e_edges = allreduce(edges_step * args.e2e_steps, dist.ReduceOp.SUM if world > 1 else None)
+        e2e = {"value": e_edges / t_e2e / 1e9, "unit": "GTEPS",
+               "h2d_bytes_per_step": 16 * (len(bfs_d) + len(sssp_d)),
+               "d2h_bytes_per_step": 4 * V * (len(bfs_d) + len(sssp_d)),
+               "steps": args.e2e_steps, "ms_per_step": 1e3 * t_e2e / args.e2e_steps,
+               "output": "pinned host buffers, vertex-major int32/uint32"}
+
+    # ---- CPU baseline (rank 0, N = 1): the reference CPU traversal, bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        nb = min(len(bfs_d), max(1, threads))
+        ns = min(len(sssp_d), max(1, threads // 2))
+        dt, edges, kind, (cb, cs) = cpu_reference_sample(g, bfs_src[:nb], sssp_src[:ns], threads)
+        hb_all = out_b[:, :nb].cpu().numpy().T
+        hs_all = out_s[:, :ns].cpu().numpy().T.view(np.uint32)
+        cs_u = np.where(np.isinf(cs), 2**32 - 1, cs).astype(np.uint32) if cs.dtype == np.float32 else cs
+        cpu = {"value": edges / dt / 1e9, "unit": "GTEPS", "cores": threads, "kind": kind,
+               "sample": f"{nb} BFS + {ns} SSSP queries of the workload, one query per thread "
+                         f"({dt:.1f} s)",
+               "matches_gpu": bool(np.array_equal(hb_all, cb) and np.array_equal(hs_all, cs_u))}
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": "aggregate GTEPS", "value": value, "unit": "GTEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup),
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": workload_name(args), "graph": "rmat", "scale": args.scale,
+                       "edge_factor": args.edge_factor, "a_b_c": [0.57, 0.19, 0.19],
+                       "V": V, "E": g.num_edges, "weights": "u32 uniform [1,64]",
+                       "queries_per_gpu": {"bfs": len(bfs_d), "sssp": len(sssp_d)},
+                       "mask_words": W, "largest_component_vertices": comp_v,
+                       "traversal_mode": args.mode,
+                       "l2": f"inputs larger than L2: CSR {4 * (V + 1 + 2 * g.num_edges) / 2**20:.0f} MiB "
+                             f"+ outputs {8 * V * (len(bfs_d) + len(sssp_d)) / 2**30:.1f} GiB "
+                             f"per step, re-initialised every step (no flush)",
+                       "parallelism": f"query-sharded x{world}"},
+            "queries_per_s": qps,
+            "bfs": {"ms": t_b / args.steps,
+                    "gteps": comp_edges * len(bfs_d) / (t_b / args.steps / 1e3) / 1e9,
+                    "iterations": rb.iterations, "push_levels": rb.push_levels,
+                    "pull_levels": rb.pull_levels},
+            "sssp": {"ms": t_s / args.steps,
+                     "gteps": comp_edges * len(sssp_d) / (t_s / args.steps / 1e3) / 1e9,
+                     "iterations": rs.iterations},
+            "one_query": one_query,
+            "batched_vs_one_query": (value / world / one_query["gteps"]) if one_query else None,
+            "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+            "cpu_baseline": cpu, "graph_gen_s": gen_s,
+        }
+        s = json.dumps(line)
+        print(s, flush=True)
+        if args.json_out:
+            Path(args.json_out).write_text(s + "\n")
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

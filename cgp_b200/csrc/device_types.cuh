@@ -1,0 +1,140 @@
+// Device-side data structures of the traversal engine, shared by every
+// translation unit (no kernels here).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace cgp {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBlock = 256;
+constexpr int kWarpsPerBlock = kBlock / 32;
+constexpr int kHeavyChunk = 2048;  // edges of a heavy vertex per CTA work item
+constexpr int kMaxW = 16;
+constexpr int kMaxPlanes = 24;
+
+enum : int32_t { kDirPush = 0, kDirPull = 1 };
+enum : int32_t { kDepthNone = 0, kDepthDirect = 1, kDepthPlanes = 2 };
+enum : int32_t { kWeightNone = 0, kWeightU32 = 1, kWeightF32 = 2 };
+
+// status bits reported back to the host
+enum : uint32_t {
+  kStatusPlanesExhausted = 1u,  // depth planes too few for the level reached
+};
+
+struct LevelProfile {
+  int32_t level;
+  int32_t dir;
+  unsigned long long frontier;      // U_l: unique frontier vertices
+  unsigned long long edges;         // D_l: their out-degree sum
+  unsigned long long next;          // U_{l+1}
+  unsigned long long active0;       // next-frontier slot bits, first word
+  unsigned long long new_pairs;     // N_l: (query, vertex) pairs newly reached (BFS bits)
+  unsigned long long pull_vertices; // P_l: vertices scanned by a pull level
+  unsigned long long pull_edges;    // S_l: in-edges read before early exit
+  unsigned long long sssp_pairs;    // A_l: (edge, active query) relaxations attempted
+  unsigned long long sssp_active;   // sum over frontier vertices of active SSSP bits
+  unsigned long long improved;      // SSSP (query, vertex) improvements
+};
+
+// Per-level work counters (reset by the level-end kernel).
+struct LevelCounters {
+  unsigned long long new_pairs;
+  unsigned long long pull_vertices;
+  unsigned long long pull_edges;
+  unsigned long long sssp_pairs;
+  unsigned long long sssp_active;
+  unsigned long long improved;
+};
+
+// Control block of one traversal group (device memory).
+struct LevelCtl {
+  unsigned long long count[2];  // unique frontier sizes by level parity
+  unsigned long long edges[2];  // sum of out-degrees of those frontiers
+  unsigned long long prev_count;
+  unsigned long long total_frontier;
+  unsigned long long total_edges;
+  uint64_t active[2][kMaxW];    // OR of the frontier masks by parity
+  uint64_t expand[kMaxW];       // bits allowed to expand at the current level
+  uint64_t bfs_bits[kMaxW];     // slots with visited-mask semantics (BFS, k-hop)
+  uint64_t sssp_bits[kMaxW];    // slots with min-reduce semantics (SSSP)
+  int32_t level;
+  int32_t dir;
+  int32_t done;
+  uint32_t status;
+  int32_t forced_dir;           // -1: decide; else direction of the next level
+  int32_t halt_level;           // stop (without converging) once level reaches it; <0 none
+  int32_t push_levels;
+  int32_t pull_levels;
+  int32_t max_iterations;       // 0: unbounded
+  int32_t mode;                 // CGP_MODE_*
+  int32_t num_planes;
+  int32_t profile_cap;
+  unsigned long long pull_vertex_threshold;
+  unsigned long long pull_edge_threshold;
+  LevelCounters lc;                // counters of the current level
+  LevelCounters total;             // sums over all levels
+};
+
+// Per-slot metadata.
+struct SlotDev {
+  int32_t kind;    // CGP_KIND_*
+  int32_t source;
+  int32_t k;       // hop bound (k-hop)
+  int32_t base;    // level at which the slot was admitted
+};
+
+struct DevGraph {
+  const void* row;       // int32 or int64 offsets (template OT)
+  const int32_t* col;
+  const void* w;
+  const void* prow;      // CSR used by pull (the transpose for directed graphs)
+  const int32_t* pcol;
+  int64_t V;
+  int64_t E;
+  const int32_t* heavy;             // vertices with out-degree > heavy_degree
+  const int64_t* heavy_chunk_start; // [n_heavy + 1] prefix of chunk counts
+  int32_t n_heavy;
+  int64_t heavy_chunks;
+  const int32_t* pheavy;            // same for the pull CSR
+  const int64_t* pheavy_chunk_start;
+  int32_t n_pheavy;
+  int64_t pheavy_chunks;
+  int64_t heavy_degree;
+};
+
+struct GroupDev {
+  uint64_t* visited;   // [V*W]
+  uint64_t* fbuf0;     // [V*W] frontier masks, level parity 0
+  uint64_t* fbuf1;
+  int32_t* list0;      // unique frontier vertex lists
+  int32_t* list1;
+  int32_t* stamp;      // last level (+1) a vertex was appended in push
+  uint64_t* planes;    // [K][V*W] depth bit planes
+  uint32_t* values;    // [V*Qg] vertex-major values (SSSP, direct depths)
+  uint64_t* hacc;      // [n_pheavy*W] pull accumulators of heavy vertices
+  LevelCtl* ctl;
+  LevelProfile* prof;
+  const SlotDev* slots;
+  int32_t Qg;
+};
+
+// Output mapping: group slot q is global query qmap[q]; element (v, gq)
+// lives at out[v*sv + gq*sq].
+struct OutMap {
+  uint32_t* out;
+  int64_t sv;
+  int64_t sq;
+  const int32_t* qmap;
+};
+
+template <typename OT>
+__device__ __forceinline__ int64_t row_at(const void* row, int64_t v) {
+  return static_cast<int64_t>(static_cast<const OT*>(row)[v]);
+}
+
+}  // namespace dev
+}  // namespace cgp

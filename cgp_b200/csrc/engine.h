@@ -1,0 +1,175 @@
+// Host-side engine structures shared by the batch runner, the enactor
+// surface and the serving loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "cgp_b200_internal.h"
+#include "device_types.cuh"
+
+namespace cgp {
+
+// Throws CudaError; caught at the C boundary and turned into CGP_ERR_CUDA/OOM.
+struct CudaError {
+  cudaError_t code;
+  std::string where;
+};
+struct ApiError {
+  cgp_status code;
+  std::string msg;
+};
+
+inline void ck(cudaError_t e, const char* where) {
+  if (e != cudaSuccess) throw CudaError{e, where};
+}
+
+// One device allocation that only grows.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf();
+  // Returns true when a new block was allocated (pointers changed).
+  bool ensure(size_t need);
+  template <typename T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+struct HeavyTable {
+  DevBuf vertices;     // int32 [n]
+  DevBuf chunk_start;  // int64 [n + 1]
+  int32_t n = 0;
+  int64_t chunks = 0;
+};
+
+using LevelCtl = dev::LevelCtl;
+
+struct CachedGraph {
+  cudaGraphExec_t exec;
+  int launches;  // kernels per replay
+};
+
+// Kernel classes timed by KernelTimer.
+enum KernelClass {
+  kClassClear = 0,
+  kClassBfsPush,
+  kClassBfsPull,
+  kClassSsspPush,
+  kClassLevelEnd,
+  kClassInit,
+  kClassOutput,
+  kClassWcc,
+  kNumClasses
+};
+
+// CUDA-event timing per kernel class on the launching stream.  mark(c)
+// closes the open interval and opens one of class c (c < 0: close only).
+struct KernelTimer {
+  static constexpr int kMaxMarks = 32;
+  cudaEvent_t ev[kMaxMarks] = {};
+  int cls[kMaxMarks] = {};
+  int n = 0;
+  double ms[kNumClasses] = {};
+  long long count[kNumClasses] = {};
+  KernelTimer();
+  ~KernelTimer();
+  void mark(int c, cudaStream_t s);
+  void flush();  // waits for the recorded events and accumulates
+};
+
+// Everything that belongs to one traversal group's device state.  Reused
+// across runs; `generation` changes whenever an allocation moves, which
+// invalidates captured CUDA graphs.
+struct Workspace {
+  int device = 0;
+  DevBuf visited, fbuf0, fbuf1, list0, list1, stamp, planes, values, hacc;
+  DevBuf ctl, prof, slots, stage, wcc, qmap;
+  LevelCtl* hctl = nullptr;  // pinned, 2 snapshots
+  dev::SlotDev* hslots = nullptr;  // pinned, kMaxWords*64 entries
+  cudaStream_t stream = nullptr;
+  cudaStream_t capture = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint64_t generation = 1;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, uint64_t, uint64_t>, CachedGraph> graphs;
+  Workspace(int dev);
+  ~Workspace();
+  void clear_graphs();
+};
+
+struct GraphImpl {
+  int device = 0;
+  int num_sms = 148;
+  int64_t V = 0, E = 0;
+  int offset_bytes = 4;
+  int weight_kind = CGP_WEIGHT_NONE;
+  bool symmetric = false;
+  DevBuf row, col, w;      // traversal CSR
+  DevBuf trow, tcol;       // transpose (in-edges) for pull on directed graphs
+  int64_t heavy_degree = 0;
+  HeavyTable heavy, pheavy;
+  std::mutex mu;
+  std::vector<std::unique_ptr<Workspace>> pool;  // idle workspaces
+
+  const void* pull_row() const { return symmetric ? row.p : trow.p; }
+  const int32_t* pull_col() const { return symmetric ? col.as<int32_t>() : tcol.as<int32_t>(); }
+  dev::DevGraph dev_graph() const;
+  void ensure_heavy(int64_t h, cudaStream_t s);
+  std::unique_ptr<Workspace> acquire();
+  void release(std::unique_ptr<Workspace> ws);
+};
+
+// A traversal group: up to 64*W slots sharing one set of vertex masks.
+struct GroupSpec {
+  int W = 1;
+  int Qg = 0;
+  std::vector<dev::SlotDev> slots;
+  int depth_mode = dev::kDepthDirect;
+  bool has_bfs = false;
+  bool has_sssp = false;
+  uint32_t* external_values = nullptr;  // caller's device buffer used as working values
+  uint64_t launches = 0;                // kernels enqueued for this group
+};
+
+struct GroupRun {
+  int32_t iterations = 0;
+  int32_t push_levels = 0;
+  int32_t pull_levels = 0;
+  uint64_t frontier_vertices = 0;
+  uint64_t frontier_edges = 0;
+  uint32_t status = 0;
+  dev::LevelCounters counters{};
+  std::vector<dev::LevelProfile> profiles;
+};
+
+// Engine entry points (engine.cu).
+GroupSpec make_group(const cgp_query* q, int n, int W, int depth_mode);
+void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
+                   cudaStream_t s);
+// Runs levels until convergence (done != 0) or, with max_levels > 0, that
+// many levels.  With a KernelTimer, levels run one at a time without graphs.
+void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
+                 cudaStream_t s, GroupRun* out, int max_levels, KernelTimer* kt = nullptr);
+void group_write_output(GraphImpl* g, Workspace* ws, GroupSpec& spec,
+                        dev::OutMap om, int query_major, cudaStream_t s);
+int choose_words(int n, int requested);
+int64_t group_state_bytes(const GraphImpl* g, int W, int Qg, int depth_mode);
+// WCC: minimum vertex id of each weak component into `labels` (device).
+void wcc_labels(GraphImpl* g, uint32_t* labels, cudaStream_t s);
+// Writes labels[v] into global column `col` of the output mapping.
+void broadcast_labels(const uint32_t* labels, int64_t V, dev::OutMap om, int col,
+                      cudaStream_t s);
+
+cgp_status translate_exception();
+
+}  // namespace cgp
+
+struct cgp_graph {
+  cgp::GraphImpl impl;
+};

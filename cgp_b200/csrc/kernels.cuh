@@ -1,0 +1,1092 @@
+// Device code of the multi-query traversal engine (sm_100a).
+//
+// One traversal group holds up to 64*W queries; every vertex carries W 64-bit
+// mask words.  Per level the host-free control block (LevelCtl) decides the
+// direction on the device, so a whole chunk of levels can be captured in one
+// CUDA graph and replayed without host synchronisation.
+//
+// Reference correspondence (paths relative to the reference project root):
+//   push  : expand_shared_node_{,warp_}kernel, frontier_engine.hxx:678-943,
+//           expand_shared_node_{,warp_}hybrid_kernel, hybrid_engine.hxx:132-330
+//   pull  : fused_ge_bfs_pull_*, frontier_engine.hxx:1561-1740 (bottom-up BFS)
+//   next-frontier marking : mark_next_shared_frontier[_with_signal],
+//           frontier_engine.hxx:117-173 (here warp-aggregated)
+//   min relaxation : apply_min_reduce, reduce_ops.hxx:40-56 (here a single
+//           atomicMin on the ordered uint32 image of the value)
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "device_types.cuh"
+
+namespace cgp {
+namespace dev {
+
+// ------------------------------------------------------------------ utils
+template <int W>
+__device__ __forceinline__ void load_mask(const uint64_t* p, uint64_t (&m)[W]) {
+  if constexpr (W % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < W; i += 2) {
+      ulonglong2 x = *reinterpret_cast<const ulonglong2*>(p + i);
+      m[i] = x.x;
+      m[i + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) m[i] = p[i];
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void store_mask(uint64_t* p, const uint64_t (&m)[W]) {
+  if constexpr (W % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < W; i += 2) {
+      *reinterpret_cast<ulonglong2*>(p + i) = make_ulonglong2(m[i], m[i + 1]);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; ++i) p[i] = m[i];
+  }
+}
+
+template <int W>
+__device__ __forceinline__ bool mask_any(const uint64_t (&m)[W]) {
+  uint64_t a = 0;
+#pragma unroll
+  for (int i = 0; i < W; ++i) a |= m[i];
+  return a != 0;
+}
+
+__device__ __forceinline__ uint64_t atomic_or64(uint64_t* p, uint64_t v) {
+  return static_cast<uint64_t>(atomicOr(reinterpret_cast<unsigned long long*>(p),
+                                        static_cast<unsigned long long>(v)));
+}
+
+// All 32 lanes call.  Lanes with `pred` append `v` to `list` (one atomicAdd
+// per warp) and add `deg` to the edge counter.
+__device__ __forceinline__ void warp_append(bool pred, int32_t v, uint64_t deg,
+                                            int32_t* list,
+                                            unsigned long long* count,
+                                            unsigned long long* edges, int lane) {
+  unsigned m = __ballot_sync(kFull, pred);
+  if (m == 0) return;
+  unsigned long long d = pred ? deg : 0ULL;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
+  int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) {
+    base = atomicAdd(count, static_cast<unsigned long long>(__popc(m)));
+    atomicAdd(edges, d);
+  }
+  base = __shfl_sync(kFull, base, leader);
+  if (pred) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// Warp-sums `x` and lane 0 adds it to *dst (all lanes call).
+__device__ __forceinline__ void warp_add(unsigned long long x, unsigned long long* dst, int lane) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  if (lane == 0 && x) atomicAdd(dst, x);
+}
+
+template <int W>
+__device__ __forceinline__ void warp_or_reduce(uint64_t (&m)[W]) {
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m[i] |= __shfl_xor_sync(kFull, m[i], o);
+  }
+}
+
+// ORs each warp's union into ctl->active[par] (lane 0, nonzero words only).
+template <int W>
+__device__ __forceinline__ void flush_union(uint64_t (&uni)[W], uint64_t* dst,
+                                            int lane) {
+  warp_or_reduce<W>(uni);
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < W; ++i)
+      if (uni[i]) atomic_or64(dst + i, uni[i]);
+  }
+}
+
+// Position of the j-th (0-based) set bit of a 64-bit word, by halving with
+// population counts.
+__device__ __forceinline__ int select_bit64(uint64_t x, int j) {
+  int pos = 0;
+  int c = __popc(static_cast<unsigned>(x));
+  if (j >= c) {
+    j -= c;
+    x >>= 32;
+    pos += 32;
+  }
+  unsigned w = static_cast<unsigned>(x);
+  c = __popc(w & 0xffffu);
+  if (j >= c) { j -= c; w >>= 16; pos += 16; }
+  c = __popc(w & 0xffu);
+  if (j >= c) { j -= c; w >>= 8; pos += 8; }
+  c = __popc(w & 0xfu);
+  if (j >= c) { j -= c; w >>= 4; pos += 4; }
+  c = __popc(w & 0x3u);
+  if (j >= c) { j -= c; w >>= 2; pos += 2; }
+  if (j >= static_cast<int>(w & 1u)) pos += 1;
+  return pos;
+}
+
+// j-th (0-based) set bit of a W-word mask.
+template <int W>
+__device__ __forceinline__ int jth_set_bit(const uint64_t* bits, int j) {
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    const int c = __popcll(bits[i]);
+    if (j < c) return i * 64 + select_bit64(bits[i], j);
+    j -= c;
+  }
+  return -1;
+}
+
+// Pointers of the current level.
+struct LevelView {
+  int level;
+  int par;
+  const int32_t* list;
+  int32_t* nlist;
+  const uint64_t* fcur;
+  uint64_t* fnext;
+  unsigned long long* ncount;
+  unsigned long long* nedges;
+  uint64_t* nactive;
+};
+
+__device__ __forceinline__ LevelView level_view(const GroupDev& g) {
+  LevelView lv;
+  lv.level = g.ctl->level;
+  lv.par = lv.level & 1;
+  lv.list = lv.par ? g.list1 : g.list0;
+  lv.nlist = lv.par ? g.list0 : g.list1;
+  lv.fcur = lv.par ? g.fbuf1 : g.fbuf0;
+  lv.fnext = lv.par ? g.fbuf0 : g.fbuf1;
+  lv.ncount = &g.ctl->count[lv.par ^ 1];
+  lv.nedges = &g.ctl->edges[lv.par ^ 1];
+  lv.nactive = g.ctl->active[lv.par ^ 1];
+  return lv;
+}
+
+// ------------------------------------------------------- depth recording
+// Records depth `depth_abs` (level + 1) for the newly visited bits `nw` of
+// vertex n: direct mode writes values[n][q] = depth_abs - base[q]; planes
+// mode ORs the bits into the planes of depth_abs's set bits.
+template <int W, int DEPTH>
+__device__ __forceinline__ void record_depth(const GroupDev& g, int64_t V,
+                                            int32_t n, const uint64_t (&nw)[W],
+                                            int depth_abs, bool exclusive) {
+  if constexpr (DEPTH == kDepthPlanes) {
+    const int K = g.ctl->num_planes;
+    for (int b = 0; b < K; ++b) {
+      if (((depth_abs >> b) & 1) == 0) continue;
+      uint64_t* p = g.planes + static_cast<size_t>(b) * static_cast<size_t>(V) * W +
+                    static_cast<size_t>(n) * W;
+#pragma unroll
+      for (int i = 0; i < W; ++i) {
+        if (!nw[i]) continue;
+        if (exclusive) p[i] |= nw[i];
+        else atomic_or64(p + i, nw[i]);
+      }
+    }
+  } else if constexpr (DEPTH == kDepthDirect) {
+    uint32_t* row = g.values + static_cast<size_t>(n) * static_cast<size_t>(g.Qg);
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      uint64_t b = nw[i];
+      while (b) {
+        int q = i * 64 + __ffsll(static_cast<long long>(b)) - 1;
+        b &= b - 1;
+        row[q] = static_cast<uint32_t>(depth_abs - g.slots[q].base);
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------- BFS push
+// One edge u->n of a push level for the visited-mask bits f of u.
+template <int W, int DEPTH>
+__device__ __forceinline__ bool bfs_visit(const GroupDev& g, int64_t V,
+                                          const LevelView& lv, int32_t n,
+                                          const uint64_t (&f)[W],
+                                          uint64_t (&uni)[W],
+                                          unsigned long long& pairs) {
+  uint64_t* vis = g.visited + static_cast<size_t>(n) * W;
+  uint64_t cur[W];
+  load_mask<W>(vis, cur);
+  uint64_t d[W];
+  uint64_t any = 0;
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    d[i] = f[i] & ~cur[i];
+    any |= d[i];
+  }
+  if (!any) return false;
+  uint64_t nw[W];
+  uint64_t anyn = 0;
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    nw[i] = 0;
+    if (d[i]) {
+      uint64_t old = atomic_or64(vis + i, d[i]);
+      nw[i] = d[i] & ~old;
+      anyn |= nw[i];
+    }
+  }
+  if (!anyn) return false;
+  uint64_t* fn = lv.fnext + static_cast<size_t>(n) * W;
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    if (nw[i]) {
+      atomic_or64(fn + i, nw[i]);
+      uni[i] |= nw[i];
+      pairs += __popcll(nw[i]);
+    }
+  }
+  record_depth<W, DEPTH>(g, V, n, nw, lv.level + 1, false);
+  return atomicMax(g.stamp + n, lv.level + 1) < lv.level + 1;
+}
+
+template <typename OT>
+__device__ __forceinline__ uint64_t degree_of(const void* row, int32_t v) {
+  return static_cast<uint64_t>(row_at<OT>(row, v + 1) - row_at<OT>(row, v));
+}
+
+// Push level, non-heavy frontier vertices: one warp per tile of 32 list
+// entries; vertices with degree > 32 are expanded by the whole warp one at a
+// time, smaller ones edge-balanced across the warp through a warp scan.
+template <int W, typename OT, int DEPTH>
+__global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPush) return;
+  const LevelView lv = level_view(g);
+  const unsigned long long n = ctl->count[lv.par];
+  uint64_t sel[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) sel[i] = ctl->bfs_bits[i] & ctl->expand[i];
+  if (!mask_any<W>(sel)) return;
+
+  __shared__ int64_t s_beg[kWarpsPerBlock][32];
+  __shared__ int32_t s_inc[kWarpsPerBlock][32];
+  __shared__ uint64_t s_f[kWarpsPerBlock][32][W];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long pairs = 0;
+
+  for (unsigned long long tile = gw; tile * 32 < n; tile += nw) {
+    const unsigned long long idx = tile * 32 + lane;
+    const bool valid = idx < n;
+    int32_t u = valid ? lv.list[idx] : 0;
+    int64_t beg = 0, end = 0;
+    uint64_t f[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) f[i] = 0;
+    if (valid) {
+      beg = row_at<OT>(G.row, u);
+      end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
+      load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, f);
+#pragma unroll
+      for (int i = 0; i < W; ++i) f[i] &= sel[i];
+    }
+    const int64_t deg = end - beg;
+    const bool work = valid && mask_any<W>(f) && deg > 0 && deg <= G.heavy_degree;
+
+    unsigned big = __ballot_sync(kFull, work && deg > 32);
+    while (big) {
+      const int src = __ffs(big) - 1;
+      big &= big - 1;
+      const int64_t bb = __shfl_sync(kFull, beg, src);
+      const int64_t be = __shfl_sync(kFull, end, src);
+      uint64_t bf[W];
+#pragma unroll
+      for (int i = 0; i < W; ++i) bf[i] = __shfl_sync(kFull, f[i], src);
+      for (int64_t e0 = bb; e0 < be; e0 += 32) {
+        const int64_t e = e0 + lane;
+        int32_t nb = 0;
+        bool app = false;
+        if (e < be) {
+          nb = G.col[e];
+          app = bfs_visit<W, DEPTH>(g, G.V, lv, nb, bf, uni, pairs);
+        }
+        warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
+                    lv.ncount, lv.nedges, lane);
+      }
+    }
+
+    int sdeg = (work && deg <= 32) ? static_cast<int>(deg) : 0;
+    int inc = sdeg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const int total = __shfl_sync(kFull, inc, 31);
+    if (total == 0) continue;
+    s_beg[wib][lane] = beg;
+    s_inc[wib][lane] = inc;
+#pragma unroll
+    for (int i = 0; i < W; ++i) s_f[wib][lane][i] = f[i];
+    __syncwarp();
+    for (int b0 = 0; b0 < total; b0 += 32) {
+      const int p = b0 + lane;
+      int32_t nb = 0;
+      bool app = false;
+      if (p < total) {
+        int lo = 0, hi = 31;
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (s_inc[wib][mid] > p) hi = mid;
+          else lo = mid + 1;
+        }
+        const int start = lo ? s_inc[wib][lo - 1] : 0;
+        const int64_t e = s_beg[wib][lo] + (p - start);
+        uint64_t of[W];
+#pragma unroll
+        for (int i = 0; i < W; ++i) of[i] = s_f[wib][lo][i];
+        nb = G.col[e];
+        app = bfs_visit<W, DEPTH>(g, G.V, lv, nb, of, uni, pairs);
+      }
+      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
+                  lv.ncount, lv.nedges, lane);
+    }
+    __syncwarp();
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(pairs, &g.ctl->lc.new_pairs, lane);
+}
+
+// Push level, heavy frontier vertices: the static heavy list is cut into
+// kHeavyChunk-edge work items spread over all CTAs.
+template <int W, typename OT, int DEPTH>
+__global__ void __launch_bounds__(kBlock) k_bfs_push_heavy(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPush || G.n_heavy == 0) return;
+  const LevelView lv = level_view(g);
+  __shared__ int32_t s_h;
+  const int lane = threadIdx.x & 31;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long pairs = 0;
+  for (int64_t c = blockIdx.x; c < G.heavy_chunks; c += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = G.n_heavy - 1;  // last h with start[h] <= c
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (G.heavy_chunk_start[mid] <= c) lo = mid;
+        else hi = mid - 1;
+      }
+      s_h = lo;
+    }
+    __syncthreads();
+    const int h = s_h;
+    __syncthreads();
+    const int32_t u = G.heavy[h];
+    uint64_t f[W];
+    load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, f);
+#pragma unroll
+    for (int i = 0; i < W; ++i) f[i] &= ctl->bfs_bits[i] & ctl->expand[i];
+    if (!mask_any<W>(f)) continue;
+    const int64_t beg = row_at<OT>(G.row, u);
+    const int64_t end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
+    const int64_t cb = beg + (c - G.heavy_chunk_start[h]) * kHeavyChunk;
+    const int64_t ce = min(end, cb + kHeavyChunk);
+    for (int64_t e0 = cb + (threadIdx.x & ~31); e0 < ce; e0 += blockDim.x) {
+      const int64_t e = e0 + lane;
+      int32_t nb = 0;
+      bool app = false;
+      if (e < ce) {
+        nb = G.col[e];
+        app = bfs_visit<W, DEPTH>(g, G.V, lv, nb, f, uni, pairs);
+      }
+      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
+                  lv.ncount, lv.nedges, lane);
+    }
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(pairs, &g.ctl->lc.new_pairs, lane);
+}
+
+// Zeroes the next-frontier buffer where the previous frontier left bits
+// (exactly the vertices of that frontier's list).  Push levels only: a pull
+// level rewrites every vertex's next mask.
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_clear_next(GroupDev g) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPush) return;
+  const LevelView lv = level_view(g);
+  const unsigned long long n = ctl->prev_count;
+  const int32_t* plist = lv.nlist;  // list of the previous frontier
+  for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+       i < n; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    uint64_t z[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) z[k] = 0;
+    store_mask<W>(lv.fnext + static_cast<size_t>(plist[i]) * W, z);
+  }
+}
+
+// --------------------------------------------------------------- BFS pull
+// Finishes one pulled vertex: writes its next mask, visited and depth.
+template <int W, int DEPTH>
+__device__ __forceinline__ void pull_commit(const GroupDev& g, int64_t V,
+                                            const LevelView& lv, int32_t v,
+                                            const uint64_t (&vis)[W],
+                                            const uint64_t (&nw)[W],
+                                            uint64_t (&uni)[W],
+                                            unsigned long long& pairs) {
+  store_mask<W>(lv.fnext + static_cast<size_t>(v) * W, nw);
+  if (!mask_any<W>(nw)) return;
+  uint64_t nv[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    nv[i] = vis[i] | nw[i];
+    uni[i] |= nw[i];
+    pairs += __popcll(nw[i]);
+  }
+  store_mask<W>(g.visited + static_cast<size_t>(v) * W, nv);
+  record_depth<W, DEPTH>(g, V, v, nw, lv.level + 1, true);
+  // a later SSSP push of the same level must not append v a second time
+  g.stamp[v] = lv.level + 1;
+}
+
+// Pull level (bottom-up): every non-heavy vertex with unvisited active bits
+// ORs the current-frontier masks of its in-neighbours until every needed bit
+// is found (early exit).  Reads only the current frontier, so depths are
+// exactly level-synchronous.
+template <int W, typename OT, int DEPTH>
+__global__ void __launch_bounds__(kBlock) k_bfs_pull(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPull) return;
+  const LevelView lv = level_view(g);
+  uint64_t act[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i)
+    act[i] = ctl->active[lv.par][i] & ctl->bfs_bits[i] & ctl->expand[i];
+  const int lane = threadIdx.x & 31;
+  const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  const unsigned long long V = static_cast<unsigned long long>(G.V);
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long pairs = 0, pverts = 0, pedges = 0;
+
+  for (unsigned long long tile = gw; tile * 32 < V; tile += nwarps) {
+    const unsigned long long vv = tile * 32 + lane;
+    const bool valid = vv < V;
+    const int32_t v = static_cast<int32_t>(valid ? vv : 0);
+    uint64_t vis[W], need[W], acc[W];
+    int64_t beg = 0, end = 0;
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      vis[i] = 0;
+      need[i] = 0;
+      acc[i] = 0;
+    }
+    if (valid) {
+      beg = row_at<OT>(G.prow, v);
+      end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+      load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
+#pragma unroll
+      for (int i = 0; i < W; ++i) need[i] = ~vis[i] & act[i];
+    }
+    const int64_t deg = end - beg;
+    const bool heavy = deg > G.heavy_degree;
+    const bool work = valid && !heavy && deg > 0 && mask_any<W>(need);
+    pverts += work ? 1 : 0;
+    if (work && deg <= 32) {
+      for (int64_t e = beg; e < end; ++e) {
+        ++pedges;
+        uint64_t fu[W];
+        load_mask<W>(lv.fcur + static_cast<size_t>(G.pcol[e]) * W, fu);
+        bool full = true;
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+          acc[i] |= fu[i] & need[i];
+          full &= acc[i] == need[i];
+        }
+        if (full) break;
+      }
+    }
+    unsigned big = __ballot_sync(kFull, work && deg > 32);
+    while (big) {
+      const int src = __ffs(big) - 1;
+      big &= big - 1;
+      const int64_t bb = __shfl_sync(kFull, beg, src);
+      const int64_t be = __shfl_sync(kFull, end, src);
+      uint64_t bn[W], a[W];
+#pragma unroll
+      for (int i = 0; i < W; ++i) {
+        bn[i] = __shfl_sync(kFull, need[i], src);
+        a[i] = 0;
+      }
+      for (int64_t e0 = bb; e0 < be; e0 += 32) {
+        const int64_t e = e0 + lane;
+        if (e < be) {
+          ++pedges;
+          uint64_t fu[W];
+          load_mask<W>(lv.fcur + static_cast<size_t>(G.pcol[e]) * W, fu);
+#pragma unroll
+          for (int i = 0; i < W; ++i) a[i] |= fu[i] & bn[i];
+        }
+        warp_or_reduce<W>(a);
+        bool full = true;
+#pragma unroll
+        for (int i = 0; i < W; ++i) full &= a[i] == bn[i];
+        if (full) break;
+      }
+      if (lane == src) {
+#pragma unroll
+        for (int i = 0; i < W; ++i) acc[i] = a[i];
+      }
+    }
+    bool app = false;
+    if (valid && !heavy) {
+      uint64_t nwm[W];
+#pragma unroll
+      for (int i = 0; i < W; ++i) nwm[i] = acc[i] & need[i];
+      pull_commit<W, DEPTH>(g, G.V, lv, v, vis, nwm, uni, pairs);
+      app = mask_any<W>(nwm);
+    }
+    warp_append(app, v, static_cast<uint64_t>(deg), lv.nlist, lv.ncount, lv.nedges, lane);
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(pairs, &g.ctl->lc.new_pairs, lane);
+  warp_add(pverts, &g.ctl->lc.pull_vertices, lane);
+  warp_add(pedges, &g.ctl->lc.pull_edges, lane);
+}
+
+// Pull level, heavy vertices: chunks of their in-edges spread over CTAs; each
+// CTA ORs its chunk into hacc[h] (skipping chunks once hacc covers the need).
+template <int W, typename OT>
+__global__ void __launch_bounds__(kBlock) k_bfs_pull_heavy(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPull || G.n_pheavy == 0) return;
+  const LevelView lv = level_view(g);
+  __shared__ int32_t s_h;
+  __shared__ int s_skip;
+  __shared__ uint64_t s_red[kWarpsPerBlock][W];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  for (int64_t c = blockIdx.x; c < G.pheavy_chunks; c += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = G.n_pheavy - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (G.pheavy_chunk_start[mid] <= c) lo = mid;
+        else hi = mid - 1;
+      }
+      s_h = lo;
+    }
+    __syncthreads();
+    const int h = s_h;
+    const int32_t v = G.pheavy[h];
+    uint64_t vis[W], need[W];
+    load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
+    bool anyneed = false;
+#pragma unroll
+    for (int i = 0; i < W; ++i) {
+      need[i] = ~vis[i] & ctl->active[lv.par][i] & ctl->bfs_bits[i] & ctl->expand[i];
+      anyneed |= need[i] != 0;
+    }
+    if (threadIdx.x == 0) {
+      bool covered = true;
+      const volatile uint64_t* ha = g.hacc + static_cast<size_t>(h) * W;
+#pragma unroll
+      for (int i = 0; i < W; ++i) covered &= (ha[i] & need[i]) == need[i];
+      s_skip = (!anyneed || covered) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_skip) continue;
+    const int64_t beg = row_at<OT>(G.prow, v);
+    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+    const int64_t cb = beg + (c - G.pheavy_chunk_start[h]) * kHeavyChunk;
+    const int64_t ce = min(end, cb + kHeavyChunk);
+    uint64_t a[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) a[i] = 0;
+    if (threadIdx.x == 0) atomicAdd(&g.ctl->lc.pull_edges, static_cast<unsigned long long>(ce - cb));
+    for (int64_t e = cb + threadIdx.x; e < ce; e += blockDim.x) {
+      uint64_t fu[W];
+      load_mask<W>(lv.fcur + static_cast<size_t>(G.pcol[e]) * W, fu);
+#pragma unroll
+      for (int i = 0; i < W; ++i) a[i] |= fu[i] & need[i];
+    }
+    warp_or_reduce<W>(a);
+    if (lane == 0) {
+#pragma unroll
+      for (int i = 0; i < W; ++i) s_red[wib][i] = a[i];
+    }
+    __syncthreads();
+    if (threadIdx.x < W) {
+      uint64_t r = 0;
+      for (int k = 0; k < kWarpsPerBlock; ++k) r |= s_red[k][threadIdx.x];
+      if (r) atomic_or64(g.hacc + static_cast<size_t>(h) * W + threadIdx.x, r);
+    }
+    __syncthreads();
+  }
+}
+
+// Commits the heavy vertices of a pull level and resets their accumulators.
+template <int W, typename OT, int DEPTH>
+__global__ void __launch_bounds__(kBlock) k_bfs_pull_heavy_commit(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPull || G.n_pheavy == 0) return;
+  const LevelView lv = level_view(g);
+  const int lane = threadIdx.x & 31;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long pairs = 0, pverts = 0;
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
+       base < G.n_pheavy; base += stride) {
+    const int64_t h = base + lane;
+    bool app = false;
+    int32_t v = 0;
+    uint64_t deg = 0;
+    if (h < G.n_pheavy) {
+      v = G.pheavy[h];
+      uint64_t vis[W], nwm[W], acc[W];
+      load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
+      load_mask<W>(g.hacc + static_cast<size_t>(h) * W, acc);
+#pragma unroll
+      for (int i = 0; i < W; ++i) {
+        nwm[i] = acc[i] & ~vis[i] & ctl->active[lv.par][i] & ctl->bfs_bits[i] & ctl->expand[i];
+        acc[i] = 0;
+      }
+      store_mask<W>(g.hacc + static_cast<size_t>(h) * W, acc);
+      bool anyneed = false;
+#pragma unroll
+      for (int i = 0; i < W; ++i)
+        anyneed |= (~vis[i] & ctl->active[lv.par][i] & ctl->bfs_bits[i] & ctl->expand[i]) != 0;
+      pverts += anyneed ? 1 : 0;
+      pull_commit<W, DEPTH>(g, G.V, lv, v, vis, nwm, uni, pairs);
+      app = mask_any<W>(nwm);
+      deg = degree_of<OT>(G.prow, v);
+    }
+    warp_append(app, v, deg, lv.nlist, lv.ncount, lv.nedges, lane);
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(pairs, &g.ctl->lc.new_pairs, lane);
+  warp_add(pverts, &g.ctl->lc.pull_vertices, lane);
+}
+
+// -------------------------------------------------------------- SSSP push
+template <int WK>
+__device__ __forceinline__ uint32_t relax(uint32_t du, const void* w, int64_t e) {
+  if constexpr (WK == kWeightF32) {
+    float r = __fadd_rn(__uint_as_float(du), static_cast<const float*>(w)[e]);
+    return __float_as_uint(r);
+  } else {
+    uint32_t wt = (WK == kWeightU32) ? static_cast<const uint32_t*>(w)[e] : 1u;
+    return du > 0xffffffffu - wt ? 0xffffffffu : du + wt;
+  }
+}
+
+// One (edge, query) relaxation: values are compared as uint32, which orders
+// non-negative floats exactly like their values (+inf = 0x7f800000).
+template <int W, int WK>
+__device__ __forceinline__ bool sssp_relax(const GroupDev& g, const LevelView& lv,
+                                           int32_t u, int32_t n, int q,
+                                           const void* w, int64_t e,
+                                           uint64_t (&uni)[W],
+                                           unsigned long long& improved) {
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  const uint32_t du = g.values[static_cast<size_t>(u) * Qg + q];
+  const uint32_t cand = relax<WK>(du, w, e);
+  uint32_t* dst = g.values + static_cast<size_t>(n) * Qg + q;
+  if (cand >= *dst) return false;
+  const uint32_t old = atomicMin(dst, cand);
+  if (cand >= old) return false;
+  const uint64_t bit = 1ULL << (q & 63);
+  atomic_or64(lv.fnext + static_cast<size_t>(n) * W + (q >> 6), bit);
+  uni[q >> 6] |= bit;
+  ++improved;
+  return atomicMax(g.stamp + n, lv.level + 1) < lv.level + 1;
+}
+
+// SSSP push over the frontier list: the (edge, active query) pairs of a tile
+// of 32 vertices are flattened and spread evenly over the warp's lanes, so a
+// vertex with k active queries and degree d costs k*d/32 warp steps.
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done) return;
+  const LevelView lv = level_view(g);
+  const unsigned long long n = ctl->count[lv.par];
+  uint64_t sel[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) sel[i] = ctl->sssp_bits[i];
+  if (!mask_any<W>(sel)) return;
+  __shared__ int64_t s_beg[kWarpsPerBlock][32];
+  __shared__ long long s_inc[kWarpsPerBlock][32];
+  __shared__ int32_t s_k[kWarpsPerBlock][32];
+  __shared__ int32_t s_u[kWarpsPerBlock][32];
+  __shared__ uint64_t s_b[kWarpsPerBlock][32][W];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long improved = 0, spairs = 0, sactive = 0;
+  for (unsigned long long tile = gw; tile * 32 < n; tile += nwarps) {
+    const unsigned long long idx = tile * 32 + lane;
+    const bool valid = idx < n;
+    int32_t u = valid ? lv.list[idx] : 0;
+    int64_t beg = 0, end = 0;
+    uint64_t b[W];
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < W; ++i) b[i] = 0;
+    if (valid) {
+      beg = row_at<OT>(G.row, u);
+      end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
+      load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
+#pragma unroll
+      for (int i = 0; i < W; ++i) {
+        b[i] &= sel[i];
+        k += __popcll(b[i]);
+      }
+    }
+    const int64_t deg = end - beg;
+    const bool work = valid && k > 0 && deg > 0 && deg <= G.heavy_degree;
+    long long wk = work ? static_cast<long long>(k) * deg : 0;
+    spairs += static_cast<unsigned long long>(wk);
+    sactive += static_cast<unsigned long long>(k);
+    long long inc = wk;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      long long t = __shfl_up_sync(kFull, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const long long total = __shfl_sync(kFull, inc, 31);
+    if (total == 0) continue;
+    s_beg[wib][lane] = beg;
+    s_inc[wib][lane] = inc;
+    s_k[wib][lane] = k;
+    s_u[wib][lane] = u;
+#pragma unroll
+    for (int i = 0; i < W; ++i) s_b[wib][lane][i] = b[i];
+    __syncwarp();
+    for (long long b0 = 0; b0 < total; b0 += 32) {
+      const long long p = b0 + lane;
+      int32_t nb = 0;
+      bool app = false;
+      if (p < total) {
+        int lo = 0, hi = 31;
+        while (lo < hi) {
+          int mid = (lo + hi) >> 1;
+          if (s_inc[wib][mid] > p) hi = mid;
+          else lo = mid + 1;
+        }
+        const long long start = lo ? s_inc[wib][lo - 1] : 0;
+        const long long local = p - start;
+        const int ko = s_k[wib][lo];
+        const long long eoff = local / ko;
+        const int j = static_cast<int>(local - eoff * ko);
+        const int q = jth_set_bit<W>(s_b[wib][lo], j);
+        const int64_t e = s_beg[wib][lo] + eoff;
+        nb = G.col[e];
+        app = sssp_relax<W, WK>(g, lv, s_u[wib][lo], nb, q, G.w, e, uni, improved);
+      }
+      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
+                  lv.ncount, lv.nedges, lane);
+    }
+    __syncwarp();
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(improved, &g.ctl->lc.improved, lane);
+  warp_add(spairs, &g.ctl->lc.sssp_pairs, lane);
+  warp_add(sactive, &g.ctl->lc.sssp_active, lane);
+}
+
+// SSSP push for heavy frontier vertices: per chunk of kHeavyChunk edges the
+// CTA lists the active query ids once and walks (edge, query) pairs.
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || G.n_heavy == 0) return;
+  const LevelView lv = level_view(g);
+  __shared__ int32_t s_h;
+  __shared__ int32_t s_k;
+  __shared__ int16_t s_q[kMaxW * 64];
+  __shared__ int32_t s_wpre[W + 1];
+  const int lane = threadIdx.x & 31;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long improved = 0;
+  for (int64_t c = blockIdx.x; c < G.heavy_chunks; c += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = G.n_heavy - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (G.heavy_chunk_start[mid] <= c) lo = mid;
+        else hi = mid - 1;
+      }
+      s_h = lo;
+    }
+    __syncthreads();
+    const int h = s_h;
+    const int32_t u = G.heavy[h];
+    uint64_t b[W];
+    load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
+#pragma unroll
+    for (int i = 0; i < W; ++i) b[i] &= ctl->sssp_bits[i];
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int i = 0; i < W; ++i) {
+        s_wpre[i] = acc;
+        acc += __popcll(b[i]);
+      }
+      s_wpre[W] = acc;
+      s_k = acc;
+    }
+    __syncthreads();
+    const int k = s_k;
+    if (k == 0) {
+      __syncthreads();
+      continue;
+    }
+    for (int t = threadIdx.x; t < W * 64; t += blockDim.x) {
+      const int i = t >> 6, bit = t & 63;
+      if ((b[i] >> bit) & 1ULL)
+        s_q[s_wpre[i] + __popcll(b[i] & ((1ULL << bit) - 1ULL))] = static_cast<int16_t>(t);
+    }
+    __syncthreads();
+    const int64_t beg = row_at<OT>(G.row, u);
+    const int64_t end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
+    const int64_t cb = beg + (c - G.heavy_chunk_start[h]) * kHeavyChunk;
+    const int64_t ce = min(end, cb + kHeavyChunk);
+    const long long pairs = static_cast<long long>(ce - cb) * k;
+    if (threadIdx.x == 0) {
+      atomicAdd(&g.ctl->lc.sssp_pairs, static_cast<unsigned long long>(pairs));
+      if (c == G.heavy_chunk_start[h]) atomicAdd(&g.ctl->lc.sssp_active, static_cast<unsigned long long>(k));
+    }
+    for (long long p0 = threadIdx.x & ~31; p0 < pairs; p0 += blockDim.x) {
+      const long long p = p0 + lane;
+      int32_t nb = 0;
+      bool app = false;
+      if (p < pairs) {
+        const long long eoff = p / k;
+        const int q = s_q[p - eoff * k];
+        const int64_t e = cb + eoff;
+        nb = G.col[e];
+        app = sssp_relax<W, WK>(g, lv, u, nb, q, G.w, e, uni, improved);
+      }
+      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
+                  lv.ncount, lv.nedges, lane);
+    }
+    __syncthreads();
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(improved, &g.ctl->lc.improved, lane);
+}
+
+// --------------------------------------------------------- level control
+__device__ __forceinline__ int32_t decide_dir(const LevelCtl* ctl, unsigned long long count,
+                                              unsigned long long edges, bool has_bfs) {
+  if (!has_bfs) return kDirPush;
+  if (ctl->forced_dir >= 0) return ctl->forced_dir;
+  if (ctl->mode == 0) return kDirPush;   // CGP_MODE_PUSH
+  if (ctl->mode == 1) return kDirPull;   // CGP_MODE_PULL
+  return (edges >= ctl->pull_edge_threshold || count >= ctl->pull_vertex_threshold)
+             ? kDirPull : kDirPush;
+}
+
+template <int W>
+__device__ __forceinline__ bool any_bits(const uint64_t* m) {
+  uint64_t a = 0;
+  for (int i = 0; i < W; ++i) a |= m[i];
+  return a != 0;
+}
+
+// Expand mask for `level`: k-hop slots stop once their depth reaches k.
+template <int W>
+__device__ void compute_expand(LevelCtl* ctl, const SlotDev* slots, int Qg, int level) {
+  for (int i = 0; i < W; ++i) ctl->expand[i] = ~0ULL;
+  for (int q = 0; q < Qg; ++q) {
+    const SlotDev s = slots[q];
+    if (s.kind == 3 && level - s.base >= s.k) ctl->expand[q >> 6] &= ~(1ULL << (q & 63));
+  }
+}
+
+// End of a level (one thread): profile, convergence, and the set-up of the
+// next level (counter reset, direction, expand mask).
+template <int W>
+__global__ void k_level_end(GroupDev g) {
+  LevelCtl* ctl = g.ctl;
+  if (ctl->done || threadIdx.x != 0) return;
+  const int l = ctl->level;
+  const int par = l & 1;
+  const unsigned long long nextc = ctl->count[par ^ 1];
+  if (g.prof != nullptr && l < ctl->profile_cap) {
+    LevelProfile p;
+    p.level = l;
+    p.dir = ctl->dir;
+    p.frontier = ctl->count[par];
+    p.edges = ctl->edges[par];
+    p.next = nextc;
+    p.active0 = ctl->active[par ^ 1][0];
+    p.new_pairs = ctl->lc.new_pairs;
+    p.pull_vertices = ctl->lc.pull_vertices;
+    p.pull_edges = ctl->lc.pull_edges;
+    p.sssp_pairs = ctl->lc.sssp_pairs;
+    p.sssp_active = ctl->lc.sssp_active;
+    p.improved = ctl->lc.improved;
+    g.prof[l] = p;
+  }
+  ctl->total.new_pairs += ctl->lc.new_pairs;
+  ctl->total.pull_vertices += ctl->lc.pull_vertices;
+  ctl->total.pull_edges += ctl->lc.pull_edges;
+  ctl->total.sssp_pairs += ctl->lc.sssp_pairs;
+  ctl->total.sssp_active += ctl->lc.sssp_active;
+  ctl->total.improved += ctl->lc.improved;
+  ctl->lc = LevelCounters{0, 0, 0, 0, 0, 0};
+  ctl->total_frontier += ctl->count[par];
+  ctl->total_edges += ctl->edges[par];
+  if (ctl->dir == kDirPush) ctl->push_levels++;
+  else ctl->pull_levels++;
+  ctl->level = l + 1;
+  if (nextc == 0 || (ctl->max_iterations > 0 && l + 1 >= ctl->max_iterations)) {
+    ctl->done = 1;
+    return;
+  }
+  ctl->prev_count = ctl->count[par];
+  ctl->count[par] = 0;
+  ctl->edges[par] = 0;
+  for (int i = 0; i < W; ++i) ctl->active[par][i] = 0;
+  compute_expand<W>(ctl, g.slots, g.Qg, l + 1);
+  ctl->dir = decide_dir(ctl, nextc, ctl->edges[par ^ 1], any_bits<W>(ctl->bfs_bits));
+  // Pauses (done = 2) leave the next level fully set up, so the host can
+  // resume by clearing `done`: depth planes hold depths < 2^num_planes, and
+  // level l+1 writes depth l+2.
+  if (ctl->num_planes > 0 && ((l + 2) >> ctl->num_planes) != 0) {
+    ctl->status |= kStatusPlanesExhausted;
+    ctl->done = 2;
+  }
+  if (ctl->halt_level >= 0 && l + 1 >= ctl->halt_level) ctl->done = 2;
+}
+
+// Seeds the sources of every slot (one block).  Level 0 starts afterwards.
+template <int W, typename OT>
+__global__ void k_seed(GroupDev g, DevGraph G) {
+  LevelCtl* ctl = g.ctl;
+  const int lane = threadIdx.x & 31;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  for (int base = threadIdx.x & ~31; base < g.Qg; base += blockDim.x) {
+    const int q = base + lane;
+    bool app = false;
+    int32_t src = 0;
+    uint64_t deg = 0;
+    if (q < g.Qg) {
+      const SlotDev s = g.slots[q];
+      if (s.kind != 2 && s.source >= 0) {  // WCC slots are not traversal slots
+        src = s.source;
+        const uint64_t bit = 1ULL << (q & 63);
+        if (s.kind != 1) atomic_or64(g.visited + static_cast<size_t>(src) * W + (q >> 6), bit);
+        atomic_or64(g.fbuf0 + static_cast<size_t>(src) * W + (q >> 6), bit);
+        if (g.values != nullptr) g.values[static_cast<size_t>(src) * g.Qg + q] = 0u;
+        uni[q >> 6] |= bit;
+        app = atomicMax(g.stamp + src, 0) < 0;
+        deg = degree_of<OT>(G.row, src);
+      }
+    }
+    warp_append(app, src, deg, g.list0, &ctl->count[0], &ctl->edges[0], lane);
+  }
+  flush_union<W>(uni, ctl->active[0], lane);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    compute_expand<W>(ctl, g.slots, g.Qg, 0);
+    ctl->dir = decide_dir(ctl, ctl->count[0], ctl->edges[0], any_bits<W>(ctl->bfs_bits));
+    if (ctl->count[0] == 0) ctl->done = 1;
+  }
+}
+
+// --------------------------------------------------------------- output
+// Fills the working values with each slot's "unreached" marker.
+__global__ void k_fill_values(uint32_t* values, const SlotDev* slots, int Qg,
+                              int64_t V, uint32_t f32_inf_for_sssp) {
+  const size_t total = static_cast<size_t>(V) * Qg;
+  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int q = static_cast<int>(i % Qg);
+    const int kind = slots[q].kind;
+    values[i] = kind == 1 ? f32_inf_for_sssp : (kind == 2 ? 0u : 0x7fffffffu);
+  }
+}
+
+
+// Depth planes -> int32 depths (INT32_MAX where the visited bit is clear).
+// Thread per (vertex, query); consecutive threads walk the contiguous axis.
+template <int W>
+__global__ void k_materialize_planes(const uint64_t* visited, const uint64_t* planes,
+                                     int K, int64_t V, int Qg, OutMap om, int query_major) {
+  const size_t total = static_cast<size_t>(V) * Qg;
+  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    int64_t v;
+    int q;
+    if (query_major) {
+      q = static_cast<int>(i / V);
+      v = static_cast<int64_t>(i % V);
+    } else {
+      v = static_cast<int64_t>(i / Qg);
+      q = static_cast<int>(i % Qg);
+    }
+    const size_t word = static_cast<size_t>(v) * W + (q >> 6);
+    const uint64_t bit = 1ULL << (q & 63);
+    uint32_t d = 0x7fffffffu;
+    if (visited[word] & bit) {
+      d = 0;
+      for (int b = 0; b < K; ++b)
+        if (planes[static_cast<size_t>(b) * V * W + word] & bit) d |= 1u << b;
+    }
+    om.out[v * om.sv + static_cast<int64_t>(om.qmap[q]) * om.sq] = d;
+  }
+}
+
+// Working values -> output mapping (skips WCC slots).
+__global__ void k_copy_values(const uint32_t* values, const SlotDev* slots, int64_t V,
+                              int Qg, OutMap om, int query_major) {
+  const size_t total = static_cast<size_t>(V) * Qg;
+  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    int64_t v;
+    int q;
+    if (query_major) {
+      q = static_cast<int>(i / V);
+      v = static_cast<int64_t>(i % V);
+    } else {
+      v = static_cast<int64_t>(i / Qg);
+      q = static_cast<int>(i % Qg);
+    }
+    if (slots[q].kind == 2) continue;
+    om.out[v * om.sv + static_cast<int64_t>(om.qmap[q]) * om.sq] =
+        values[static_cast<size_t>(v) * Qg + q];
+  }
+}
+
+}  // namespace dev
+}  // namespace cgp

@@ -1,0 +1,335 @@
+"""Parity of the CUDA path with the CPU oracle, through the C ABI.
+
+Bit-exact everywhere: int32 BFS / k-hop depths, uint32 or float32 SSSP
+distances (compared with ==), uint32 WCC labels.
+"""
+import numpy as np
+import pytest
+
+import cgp_b200 as cgp
+import oracle
+from conftest import as_expected, host_csr
+
+pytestmark = pytest.mark.gpu
+INF = 2**31 - 1
+
+
+@pytest.fixture(scope="module")
+def rmat_u32():
+    g = cgp.gen_rmat(12, 8, seed=101).with_weights("u32", 1, 64, seed=102)
+    return g, cgp.CsrGraph(g)
+
+
+@pytest.fixture(scope="module")
+def rmat_f32():
+    g = cgp.gen_rmat(11, 8, seed=103).with_weights("f32", 1.0, 100.0, seed=104)
+    return g, cgp.CsrGraph(g)
+
+
+@pytest.fixture(scope="module")
+def grid_f32():
+    g = cgp.gen_grid(40, 50, 0.1, 0.01, seed=105).with_weights("f32", 1.0, 100.0, seed=106)
+    return g, cgp.CsrGraph(g)
+
+
+def _bfs(descs_src, graph, opts, layout="query"):
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "bfs") for s in descs_src], opts,
+                      layout=layout)
+    return r
+
+
+@pytest.mark.parametrize("nq", [1, 5, 64, 65, 130, 256])
+@pytest.mark.parametrize("mode", ["push", "pull", "hybrid"])
+def test_bfs_parity(rmat_u32, nq, mode):
+    g, graph = rmat_u32
+    src = g.pick_sources(nq, seed=nq)
+    ref, _ = oracle.batch("bfs", g, src)
+    r = _bfs(src, graph, cgp.RunOptions(traversal_mode=mode))
+    assert r.values.dtype == np.int32
+    np.testing.assert_array_equal(r.values, ref)
+    if mode == "push":
+        assert r.pull_levels == 0
+    if mode == "pull":
+        assert r.push_levels == 0
+
+
+@pytest.mark.parametrize("depth", ["planes", "direct"])
+@pytest.mark.parametrize("layout", ["vertex", "query"])
+def test_bfs_depth_modes_and_layouts(rmat_u32, depth, layout):
+    g, graph = rmat_u32
+    src = g.pick_sources(100, seed=7)
+    ref, _ = oracle.batch("bfs", g, src)
+    r = _bfs(src, graph, cgp.RunOptions(depth_mode=depth), layout=layout)
+    got = r.values if layout == "query" else r.values.T
+    np.testing.assert_array_equal(got, ref)
+    assert r.depth_mode == depth
+
+
+@pytest.mark.parametrize("opts", [
+    dict(use_cuda_graph=False), dict(levels_per_sync=1), dict(levels_per_sync=3),
+    dict(heavy_degree=16), dict(heavy_degree=64, traversal_mode="pull"),
+    dict(mask_words=16), dict(pull_edge_ratio=0.0, pull_frontier_ratio=0.0),
+])
+def test_bfs_execution_knobs_do_not_change_results(rmat_u32, opts):
+    g, graph = rmat_u32
+    src = g.pick_sources(70, seed=3)
+    ref, _ = oracle.batch("bfs", g, src)
+    r = _bfs(src, graph, cgp.RunOptions(**opts))
+    np.testing.assert_array_equal(r.values, ref)
+
+
+def test_bfs_multiple_groups(rmat_u32):
+    g, graph = rmat_u32
+    src = g.pick_sources(1100, seed=9)
+    ref, _ = oracle.batch("bfs", g, src)
+    r = _bfs(src, graph, cgp.RunOptions())
+    assert r.groups == 2
+    np.testing.assert_array_equal(r.values, ref)
+
+
+def test_bfs_int64_offsets():
+    g = cgp.gen_rmat(11, 8, seed=33)
+    graph = cgp.CsrGraph(g, offsets64=True)
+    src = g.pick_sources(40, seed=4)
+    ref, _ = oracle.batch("bfs", g, src)
+    np.testing.assert_array_equal(_bfs(src, graph, cgp.RunOptions()).values, ref)
+
+
+def test_bfs_deep_graph_grows_depth_planes():
+    n = 700  # depth 699 needs 10 depth planes; the engine starts with 8
+    g = cgp.csr_from_edges(n, list(range(n - 1)), list(range(1, n)))
+    graph = cgp.CsrGraph(g)
+    src = [0, 350, 699] * 6
+    ref, _ = oracle.batch("bfs", g, src)
+    r = _bfs(src, graph, cgp.RunOptions(depth_mode="planes"))
+    np.testing.assert_array_equal(r.values, ref)
+    assert r.iterations >= 699
+
+
+def test_bfs_directed_graph_pull_uses_transpose():
+    rng = np.random.default_rng(5)
+    V = 3000
+    s = rng.integers(0, V, 20000)
+    d = rng.integers(0, V, 20000)
+    g = cgp.csr_from_edges(V, s, d, symmetrize=False)
+    graph = cgp.CsrGraph(g)
+    assert not graph.symmetric
+    src = g.pick_sources(50, seed=6)
+    ref, _ = oracle.batch("bfs", g, src)
+    for mode in ("push", "pull", "hybrid"):
+        np.testing.assert_array_equal(_bfs(src, graph, cgp.RunOptions(traversal_mode=mode)).values, ref)
+
+
+@pytest.mark.parametrize("nq", [1, 33, 64, 200])
+def test_sssp_u32_parity(rmat_u32, nq):
+    g, graph = rmat_u32
+    src = g.pick_sources(nq, seed=50 + nq)
+    ref, _ = oracle.batch("sssp", g, src)
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src], layout="query")
+    assert r.values.dtype == np.uint32
+    np.testing.assert_array_equal(r.values, ref)
+
+
+@pytest.mark.parametrize("which", ["rmat", "grid"])
+def test_sssp_f32_parity(rmat_f32, grid_f32, which):
+    g, graph = rmat_f32 if which == "rmat" else grid_f32
+    src = g.pick_sources(80, seed=12)
+    ref, _ = oracle.batch("sssp", g, src)
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src], layout="query")
+    assert r.values.dtype == np.float32
+    np.testing.assert_array_equal(r.values, ref)  # exact: least fixpoint of fp32 left folds
+
+
+def test_sssp_heavy_paths(rmat_u32):
+    g, graph = rmat_u32
+    src = g.pick_sources(90, seed=77)
+    ref, _ = oracle.batch("sssp", g, src)
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                      cgp.RunOptions(heavy_degree=8), layout="query")
+    np.testing.assert_array_equal(r.values, ref)
+
+
+def test_wcc_parity(rmat_u32, grid_f32):
+    for g, graph in (rmat_u32, grid_f32):
+        r = cgp.run("wcc", graph, [0])
+        np.testing.assert_array_equal(r.values[:, 0], oracle.wcc_components(g))
+        np.testing.assert_array_equal(r.values[:, 0], oracle.wcc_label_propagation(g))
+
+
+def test_khop_parity(rmat_u32):
+    g, graph = rmat_u32
+    src = g.pick_sources(60, seed=14)
+    ks = [2 + (i % 5) for i in range(60)]
+    ref, _ = oracle.batch("khop", g, src, khop=ks)
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "khop", k) for s, k in zip(src, ks)],
+                      layout="query")
+    np.testing.assert_array_equal(r.values, ref)
+
+
+@pytest.mark.parametrize("mode", ["push", "hybrid"])
+def test_mixed_batch_parity(rmat_u32, mode):
+    g, graph = rmat_u32
+    src = g.pick_sources(150, seed=15)
+    kinds = ["bfs", "sssp", "khop", "wcc", "bfs", "sssp"]
+    descs = [cgp.QueryDescriptor(int(s), kinds[i % 6], 3) for i, s in enumerate(src)]
+    r = cgp.run_heterogeneous(graph, cgp.HybridQueryBatch(descs),
+                              options=cgp.RunOptions(traversal_mode=mode), layout="query")
+    wcc = oracle.wcc_components(g)
+    for i, d in enumerate(descs):
+        if d.kind == "bfs":
+            np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source))
+        elif d.kind == "khop":
+            np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source, 3))
+        elif d.kind == "sssp":
+            np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
+        else:
+            np.testing.assert_array_equal(r.values[i], wcc)
+
+
+def test_device_output_buffer(rmat_u32):
+    import torch
+    g, graph = rmat_u32
+    src = g.pick_sources(64, seed=16)
+    ref, _ = oracle.batch("bfs", g, src)
+    out = torch.empty((g.num_vertices, 64), dtype=torch.int32, device="cuda")
+    cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "bfs") for s in src], out=out)
+    np.testing.assert_array_equal(out.cpu().numpy().T, ref)
+
+
+def test_repeat_runs_are_deterministic(rmat_u32):
+    g, graph = rmat_u32
+    src = g.pick_sources(64, seed=17)
+    a = _bfs(src, graph, cgp.RunOptions()).values
+    b = _bfs(src, graph, cgp.RunOptions()).values
+    assert np.array_equal(a, b)
+
+
+# ------------------------------------------------ reference known answers
+def _case(golden, name):
+    return next(c for c in golden["cases"] if c["name"] == name)
+
+
+def _typed(kind, vec, graph):
+    """Expected 4-byte words: SSSP is float32 on float-weighted graphs and
+    uint32 (UINT32_MAX unreached) otherwise; BFS int32; WCC uint32."""
+    if kind == "sssp":
+        f = as_expected(vec, np.float32)
+        if graph.weight_kind == 2:
+            return f.view(np.uint32)
+        return np.where(np.isinf(f), 2**32 - 1, f).astype(np.uint32)
+    return np.asarray(vec, np.int64).astype(np.uint32)
+
+
+@pytest.mark.parametrize("name", ["hybrid_toy", "replenish_toy", "wcc_toy"])
+def test_reference_known_answers(golden, name):
+    c = _case(golden, name)
+    g = host_csr(c["graph"])
+    graph = cgp.CsrGraph(g)
+    descs = [cgp.QueryDescriptor(s, k) for k, s in c["queries"]]
+    r = cgp.run_batch(graph, descs, cgp.RunOptions(traversal_mode="push"), layout="query")
+    for i, ((k, _), exp) in enumerate(zip(c["queries"], c["expect"])):
+        np.testing.assert_array_equal(r.values[i], _typed(k, exp, graph))
+
+
+def test_reference_mm_fixtures(golden):
+    for name in ("unweighted_mm", "weighted_mm"):
+        c = _case(golden, name)
+        g = host_csr(c["graph"])
+        graph = cgp.CsrGraph(g)
+        kind = c["kind"]
+        r = cgp.run(kind, graph, c["sources"])
+        for i, exp in enumerate(c["expect"]):
+            got = r.values[:, i]
+            if kind == "bfs":
+                assert got.tolist() == exp
+            else:
+                np.testing.assert_array_equal(got, as_expected(exp, np.float32))
+
+
+@pytest.mark.parametrize("name", ["rmat8_ref", "grid12_ref"])
+def test_reference_outputs_on_seeded_graphs(golden, name):
+    c = _case(golden, name)
+    g = host_csr(c["graph"])
+    graph = cgp.CsrGraph(g)
+    rb = cgp.run("bfs", graph, c["sources"])
+    rs = cgp.run("sssp", graph, c["sources"])
+    for i in range(len(c["sources"])):
+        assert rb.values[:, i].tolist() == c["bfs"][i]
+        np.testing.assert_array_equal(rs.values[:, i], as_expected(c["sssp"][i], np.float32))
+    rw = cgp.run("wcc", graph, [0])
+    np.testing.assert_array_equal(rw.values[:, 0], np.asarray(c["wcc"], np.float32).astype(np.uint32))
+
+
+def test_one_push_level_like_smoke_hybrid_push(golden):
+    c = _case(golden, "push_one_level")
+    g = host_csr(c["graph"])
+    graph = cgp.CsrGraph(g)
+    descs = [cgp.QueryDescriptor(s, k) for k, s in c["queries"]]
+    e = cgp.Enactor(graph, descs, cgp.RunOptions(traversal_mode="push", depth_mode="direct"))
+    e.prepare_frontier()
+    n = e.loop("push")
+    vs, ms = e.frontier()
+    assert n == 2 and sorted(vs.tolist()) == c["expect_next_frontier"]["vertices"]
+    assert all(int(m[0]) == c["expect_next_frontier"]["mask"] for m in ms)
+    vals = e.values("query")
+    for i, ((k, _), exp) in enumerate(zip(c["queries"], c["expect"])):
+        np.testing.assert_array_equal(vals[i], _typed(k, exp, graph))
+    assert not e.is_converged()
+    while not e.is_converged():
+        e.loop("hybrid")
+    e.close()
+
+
+def test_prepare_frontier_like_smoke_hybrid_init(golden):
+    c = _case(golden, "hybrid_init")
+    g = host_csr(c["graph"])
+    graph = cgp.CsrGraph(g)
+    descs = [cgp.QueryDescriptor(s, k) for k, s in c["queries"]]
+    e = cgp.Enactor(graph, descs, cgp.RunOptions(depth_mode="direct"))
+    e.prepare_frontier()
+    vs, ms = e.frontier()
+    got = {str(int(v)): int(m[0]) for v, m in zip(vs, ms)}
+    assert got == c["expect_frontier"]
+    vals = e.values("query")
+    for i, ((k, _), exp) in enumerate(zip(c["queries"], c["expect"])):
+        np.testing.assert_array_equal(vals[i], _typed(k, exp, graph))
+
+
+def test_convergence_masks_like_smoke_replenish(golden):
+    c = _case(golden, "convergence_levels")
+    g = host_csr(c["graph"])
+    graph = cgp.CsrGraph(g)
+    descs = [cgp.QueryDescriptor(s, k) for k, s in c["queries"]]
+    r = cgp.run_batch(graph, descs, cgp.RunOptions(traversal_mode="push", profile_iterations=True))
+    assert r.iterations == c["expect_iterations"]
+    masks = [p.query_convergence_mask for p in r.iteration_profiles]
+    assert masks == c["expect_masks"]
+    for a, b in zip(masks, masks[1:]):
+        assert b & ~a == 0  # monotone
+
+
+def test_enactor_steps_equal_enact(rmat_u32):
+    g, graph = rmat_u32
+    src = g.pick_sources(100, seed=19)
+    descs = [cgp.QueryDescriptor(int(s), "bfs") for s in src]
+    e = cgp.Enactor(graph, descs)
+    e.prepare_frontier()
+    steps = 0
+    while not e.is_converged():
+        e.loop("pull" if steps % 2 else "push")
+        steps += 1
+    ref, _ = oracle.batch("bfs", g, src)
+    np.testing.assert_array_equal(e.values("query").view(np.int32), ref)
+    e.prepare_frontier()
+    e.enact()
+    np.testing.assert_array_equal(e.values("query").view(np.int32), ref)
+
+
+def test_invalid_batches_raise(rmat_u32):
+    g, graph = rmat_u32
+    with pytest.raises(ValueError):
+        cgp.run("bfs", graph, [])
+    with pytest.raises(ValueError):
+        cgp.run("bfs", graph, [g.num_vertices])
+    with pytest.raises(ValueError):
+        cgp.run("bfs", graph, [1, 2, 3], options=cgp.RunOptions(max_queries=2))
