@@ -518,3 +518,131 @@ class Enactor:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ serving
+STATE_NAMES = {0: "queued", 1: "running", 2: "done", 3: "cancelled", 4: "failed"}
+
+
+@dataclass
+class RequestInfo:
+    """Per-request record (query_result_t, core/result.hxx:13-19, plus times)."""
+    ticket: int
+    state: str
+    slot: int
+    admit_level: int
+    completion_level: int
+    submit_ms: float
+    admit_ms: float
+    finish_ms: float
+
+    @property
+    def latency_ms(self) -> float:
+        return self.finish_ms - self.submit_ms
+
+
+class Server:
+    """Continuous-batching query server (replenish_frontier_engine,
+    replenish_engine.hxx:42-554): requests are admitted into free bitmask
+    slots at level boundaries while others run; results land in the buffer
+    given at submit time."""
+
+    def __init__(self, graph: CsrGraph, slots: int = 64, options: RunOptions | None = None,
+                 max_state_bytes: int = 0):
+        self.graph = graph
+        o = (options or RunOptions()).to_c()
+        h = ctypes.c_void_p()
+        N.check(N.lib().cgp_server_create(graph.handle, slots, ctypes.byref(o), max_state_bytes,
+                                          ctypes.byref(h)), "cgp_server_create")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, desc: QueryDescriptor, out=None) -> int:
+        """Queues a request; `out` is a host numpy array / pinned tensor or a
+        device tensor of V 4-byte values, or None (result discarded)."""
+        q = _queries_c([desc])
+        t = ctypes.c_uint64()
+        ptr, on_dev = None, 0
+        if out is not None:
+            if hasattr(out, "data_ptr"):
+                ptr, on_dev = out.data_ptr(), int(bool(getattr(out, "is_cuda", False)))
+            else:
+                ptr = out.ctypes.data
+        N.check(N.lib().cgp_server_submit(self._h, q, ptr, on_dev, ctypes.byref(t)), "submit")
+        if out is not None:
+            self._keep[t.value] = out
+        return t.value
+
+    def _info(self, t, i) -> RequestInfo:
+        return RequestInfo(t, STATE_NAMES.get(i.state, "?"), i.slot, i.admit_level,
+                           i.completion_level, i.submit_time_ms, i.admit_time_ms,
+                           i.finish_time_ms)
+
+    def poll(self, ticket: int) -> RequestInfo:
+        i = N.CgpRequestInfo()
+        N.check(N.lib().cgp_server_poll(self._h, ticket, ctypes.byref(i)), "poll")
+        return self._info(ticket, i)
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> RequestInfo:
+        i = N.CgpRequestInfo()
+        N.check(N.lib().cgp_server_wait(self._h, ticket, timeout_ms, ctypes.byref(i)), "wait")
+        self._keep.pop(ticket, None)
+        return self._info(ticket, i)
+
+    def cancel(self, ticket: int) -> None:
+        N.check(N.lib().cgp_server_cancel(self._h, ticket), "cancel")
+
+    def drain(self, timeout_ms: int = -1) -> None:
+        N.check(N.lib().cgp_server_drain(self._h, timeout_ms), "drain")
+
+    def stats(self) -> dict:
+        s = N.CgpServerStats()
+        N.check(N.lib().cgp_server_get_stats(self._h, ctypes.byref(s)), "stats")
+        return {k: getattr(s, k) for k, _ in N.CgpServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().cgp_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_replenish_pipeline(graph: CsrGraph, queries: Sequence[QueryDescriptor], context=None,
+                           options: RunOptions | None = None, slots: int = 64) -> RunResult:
+    """run_replenish_pipeline (replenish_engine.hxx:559-573): all N queries
+    through `slots` bitmask slots, slots reused as queries converge.  Values
+    are row-major [N][V] like the reference's final buffer; queries carries
+    one RequestInfo per query (completion level and wall time)."""
+    options = options or RunOptions()
+    queries = list(queries)
+    if not queries:
+        raise ValueError("replenish: query list must be non-empty")
+    if not options.enable_replenishment:
+        if len(queries) > 1024:
+            raise ValueError("enable_replenishment=false but query count > 1024")
+        return run_heterogeneous(graph, HybridQueryBatch(queries), options=options, layout="query")
+    V = graph.num_vertices
+    vals = np.empty((len(queries), V), np.uint32)
+    t0 = __import__("time").perf_counter()
+    with Server(graph, min(slots, len(queries)), options) as s:
+        tickets = [s.submit(q, None if options.discard_results else vals[i])
+                   for i, q in enumerate(queries)]
+        s.drain()
+        infos = [s.wait(t) for t in tickets]
+    wall = (__import__("time").perf_counter() - t0) * 1e3
+    res = RunResult(values=vals, iterations=max(i.admit_level + i.completion_level for i in infos),
+                    gpu_time_ms=0.0, wall_time_ms=wall, effective_query_dim=len(queries),
+                    options=options)
+    res.queries = infos
+    return res

@@ -8,6 +8,7 @@ written next to this file, so it travels with the working tree.
 from __future__ import annotations
 
 import concurrent.futures
+import hashlib
 import os
 import shutil
 import subprocess
@@ -20,6 +21,7 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 BUILD = ROOT / "_build"
 LIB = PKG / "libcgp_b200.so"
+STAMP = PKG / "libcgp_b200.so.sha256"
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
@@ -64,8 +66,21 @@ def _compile(src: Path, verbose: bool) -> Path:
     return obj
 
 
+def _digest() -> str:
+    h = hashlib.sha256()
+    for f in [*_sources(), *_headers()]:
+        h.update(f.name.encode())
+        h.update(f.read_bytes())
+    h.update(" ".join(CU_FLAGS + CXX_FLAGS).encode())
+    return h.hexdigest()
+
+
 def build(verbose: bool = False, jobs: int | None = None) -> Path:
-    """Compiles every source that changed and links the shared library."""
+    """Compiles every source that changed and links the shared library.
+    A library whose recorded source digest matches is left as it is."""
+    digest = _digest()
+    if LIB.exists() and STAMP.exists() and STAMP.read_text().strip() == digest:
+        return LIB
     BUILD.mkdir(exist_ok=True)
     srcs = _sources()
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
@@ -81,6 +96,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         if r.returncode != 0:
             raise RuntimeError(f"linking failed:\n{r.stdout}\n{r.stderr}")
         shutil.move(str(tmp), str(LIB))
+    STAMP.write_text(digest + "\n")
     return LIB
 
 

@@ -475,7 +475,8 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   if (spec.depth_mode != kDepthPlanes) {
     int blocks = g->num_sms * 8;
     k_fill_values<<<blocks, kBlock, 0, s>>>(group_dev(ws, spec, false).values,
-                                            ws->slots.as<SlotDev>(), spec.Qg, V, sssp_inf);
+                                            ws->slots.as<SlotDev>(), spec.Qg, V, sssp_inf,
+                                            spec.uniform_inf);
     ck(cudaGetLastError(), "fill values");
     spec.launches++;
   }

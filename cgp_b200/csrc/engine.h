@@ -134,6 +134,7 @@ struct GroupSpec {
   bool has_bfs = false;
   bool has_sssp = false;
   uint32_t* external_values = nullptr;  // caller's device buffer used as working values
+  uint32_t uniform_inf = 0;             // nonzero: fill every value with it (serving)
   uint64_t launches = 0;                // kernels enqueued for this group
 };
 

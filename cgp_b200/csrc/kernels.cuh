@@ -966,19 +966,21 @@ __global__ void k_level_end(GroupDev g) {
   if (ctl->dir == kDirPush) ctl->push_levels++;
   else ctl->pull_levels++;
   ctl->level = l + 1;
-  if (nextc == 0 || (ctl->max_iterations > 0 && l + 1 >= ctl->max_iterations)) {
-    ctl->done = 1;
-    return;
-  }
+  // Set up level l+1 even when it is empty, so that a serving loop can add
+  // sources to it and resume.
   ctl->prev_count = ctl->count[par];
   ctl->count[par] = 0;
   ctl->edges[par] = 0;
   for (int i = 0; i < W; ++i) ctl->active[par][i] = 0;
   compute_expand<W>(ctl, g.slots, g.Qg, l + 1);
   ctl->dir = decide_dir(ctl, nextc, ctl->edges[par ^ 1], any_bits<W>(ctl->bfs_bits));
-  // Pauses (done = 2) leave the next level fully set up, so the host can
-  // resume by clearing `done`: depth planes hold depths < 2^num_planes, and
-  // level l+1 writes depth l+2.
+  if (nextc == 0 || (ctl->max_iterations > 0 && l + 1 >= ctl->max_iterations)) {
+    ctl->done = 1;
+    return;
+  }
+  // Pauses (done = 2): depth planes hold depths < 2^num_planes and level l+1
+  // writes depth l+2; or the caller asked to stop at halt_level.  The host
+  // resumes by clearing `done`.
   if (ctl->num_planes > 0 && ((l + 2) >> ctl->num_planes) != 0) {
     ctl->status |= kStatusPlanesExhausted;
     ctl->done = 2;
@@ -1025,12 +1027,18 @@ __global__ void k_seed(GroupDev g, DevGraph G) {
 }
 
 // --------------------------------------------------------------- output
-// Fills the working values with each slot's "unreached" marker.
-__global__ void k_fill_values(uint32_t* values, const SlotDev* slots, int Qg,
-                              int64_t V, uint32_t f32_inf_for_sssp) {
+// Fills the working values with each slot's "unreached" marker, or with
+// `uniform` everywhere when it is nonzero (the serving layout, where a slot
+// changes kind between requests).
+static __global__ void k_fill_values(uint32_t* values, const SlotDev* slots, int Qg,
+                              int64_t V, uint32_t f32_inf_for_sssp, uint32_t uniform) {
   const size_t total = static_cast<size_t>(V) * Qg;
   for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    if (uniform) {
+      values[i] = uniform;
+      continue;
+    }
     const int q = static_cast<int>(i % Qg);
     const int kind = slots[q].kind;
     values[i] = kind == 1 ? f32_inf_for_sssp : (kind == 2 ? 0u : 0x7fffffffu);
@@ -1068,7 +1076,7 @@ __global__ void k_materialize_planes(const uint64_t* visited, const uint64_t* pl
 }
 
 // Working values -> output mapping (skips WCC slots).
-__global__ void k_copy_values(const uint32_t* values, const SlotDev* slots, int64_t V,
+static __global__ void k_copy_values(const uint32_t* values, const SlotDev* slots, int64_t V,
                               int Qg, OutMap om, int query_major) {
   const size_t total = static_cast<size_t>(V) * Qg;
   for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;

@@ -1,0 +1,646 @@
+// Continuous-batching server over one traversal group of bitmask slots.
+//
+// Replaces replenish_frontier_engine / run_replenish_pipeline
+// (puercgp/include/puercgp/engine/replenish_engine.hxx:42-573).  The
+// reference takes all N queries up front and, after every level, detects
+// converged slots from the active-slot union, snapshots them into a row-major
+// buffer, clears them and injects the next pending query.  Here requests
+// arrive at any time through cgp_server_submit; a host thread admits them
+// into free slots at level boundaries while the others keep running, retires
+// converged slots (snapshot + reset in one pass over V), and records per
+// request submit / admit / finish times.  Differences that fix reference
+// hazards: every slot has its own base level, so a BFS admitted at level L
+// writes depth = level + 1 - L (the reference writes the global level,
+// hybrid_engine.hxx:175); WCC requests are answered from one union-find pass
+// instead of occupying a slot; slot state uses one "unreached" word
+// (0xffffffff) for every kind, mapped to the kind's marker on retire.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+#include "engine.h"
+#include "kernels.cuh"
+
+namespace cgp {
+namespace {
+
+using namespace dev;
+
+constexpr uint32_t kServeInf = 0xffffffffu;
+constexpr int kRetireBatch = 32;
+
+struct AdmitReq {
+  int32_t slot;
+  int32_t kind;
+  int32_t source;
+  int32_t k;
+};
+
+struct RetireReq {
+  int32_t slot;
+  int32_t kind;
+  int32_t has_out;
+  int32_t reserved;
+};
+
+// Seeds newly admitted slots into the frontier of the current level (one
+// block, between levels).
+template <int W, typename OT>
+__global__ void k_admit(GroupDev g, DevGraph G, const AdmitReq* reqs, int n) {
+  LevelCtl* ctl = g.ctl;
+  const int L = ctl->level;
+  const int par = L & 1;
+  uint64_t* fcur = par ? g.fbuf1 : g.fbuf0;
+  int32_t* list = par ? g.list1 : g.list0;
+  SlotDev* slots = const_cast<SlotDev*>(g.slots);
+  const int lane = threadIdx.x & 31;
+  for (int base = threadIdx.x & ~31; base < n; base += blockDim.x) {
+    const int i = base + lane;
+    bool app = false;
+    int32_t src = 0;
+    uint64_t deg = 0;
+    if (i < n) {
+      const AdmitReq r = reqs[i];
+      const int s = r.slot;
+      const int w = s >> 6;
+      const uint64_t bit = 1ULL << (s & 63);
+      SlotDev sd;
+      sd.kind = r.kind;
+      sd.source = r.source;
+      sd.k = r.k;
+      sd.base = L;
+      slots[s] = sd;
+      const bool bfs_like = r.kind == 0 || r.kind == 3;
+      if (bfs_like) {
+        atomic_or64(&ctl->bfs_bits[w], bit);
+        atomicAnd(reinterpret_cast<unsigned long long*>(&ctl->sssp_bits[w]), ~bit);
+        atomic_or64(g.visited + static_cast<size_t>(r.source) * W + w, bit);
+      } else {
+        atomic_or64(&ctl->sssp_bits[w], bit);
+        atomicAnd(reinterpret_cast<unsigned long long*>(&ctl->bfs_bits[w]), ~bit);
+      }
+      if (r.kind == 3 && r.k <= 0)
+        atomicAnd(reinterpret_cast<unsigned long long*>(&ctl->expand[w]), ~bit);
+      else
+        atomic_or64(&ctl->expand[w], bit);
+      g.values[static_cast<size_t>(r.source) * g.Qg + s] = 0u;
+      atomic_or64(fcur + static_cast<size_t>(r.source) * W + w, bit);
+      atomic_or64(&ctl->active[par][w], bit);
+      src = r.source;
+      app = atomicMax(g.stamp + src, L) < L;
+      deg = degree_of<OT>(G.row, src);
+    }
+    warp_append(app, src, deg, list, &ctl->count[par], &ctl->edges[par], lane);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0 && ctl->count[par] > 0) {
+    ctl->done = 0;
+    ctl->dir = decide_dir(ctl, ctl->count[par], ctl->edges[par], any_bits<W>(ctl->bfs_bits));
+  }
+}
+
+// Retires slots: snapshot each slot column (mapped to its kind's unreached
+// marker) into staging row i, reset the column, and clear the slots' visited
+// bits (and frontier bits when a running request was cancelled).
+template <int W>
+__global__ void k_retire(GroupDev g, int64_t V, const RetireReq* reqs, int n,
+                         uint32_t* staging, const uint64_t* clear, int clear_frontier,
+                         uint32_t f32) {
+  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
+       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t* row = g.values + static_cast<size_t>(v) * g.Qg;
+    for (int i = 0; i < n; ++i) {
+      const RetireReq r = reqs[i];
+      uint32_t x = row[r.slot];
+      row[r.slot] = kServeInf;
+      if (r.has_out) {
+        if (x == kServeInf) {
+          if (r.kind == 0 || r.kind == 3) x = 0x7fffffffu;
+          else if (f32) x = 0x7f800000u;
+        }
+        staging[static_cast<size_t>(i) * V + v] = x;
+      }
+    }
+    uint64_t* vis = g.visited + static_cast<size_t>(v) * W;
+    for (int w = 0; w < W; ++w) {
+      if (!clear[w]) continue;
+      vis[w] &= ~clear[w];
+      if (clear_frontier) {
+        g.fbuf0[static_cast<size_t>(v) * W + w] &= ~clear[w];
+        g.fbuf1[static_cast<size_t>(v) * W + w] &= ~clear[w];
+      }
+    }
+  }
+}
+
+template <int W, typename OT>
+void launch_admit(const GroupDev& g, const DevGraph& G, const AdmitReq* r, int n, cudaStream_t s) {
+  k_admit<W, OT><<<1, kBlock, 0, s>>>(g, G, r, n);
+}
+
+template <int W>
+void launch_retire(const GroupDev& g, int64_t V, const RetireReq* r, int n, uint32_t* st,
+                   const uint64_t* clear, int cf, uint32_t f32, int blocks, cudaStream_t s) {
+  k_retire<W><<<blocks, kBlock, 0, s>>>(g, V, r, n, st, clear, cf, f32);
+}
+
+struct Request {
+  cgp_query q{};
+  void* out = nullptr;
+  bool out_dev = false;
+  int state = 0;  // 0 queued, 1 running, 2 done, 3 cancelled, 4 failed
+  int slot = -1;
+  int admit_level = -1;
+  int completion_level = -1;
+  double t_submit = 0, t_admit = 0, t_finish = 0;
+  bool cancel = false;
+};
+
+}  // namespace
+}  // namespace cgp
+
+using namespace cgp;
+using namespace cgp::dev;
+
+struct cgp_server {
+  GraphImpl* g = nullptr;
+  cgp_options o{};
+  int S = 0;
+  int W = 1;
+  std::unique_ptr<Workspace> ws;
+  GroupSpec spec;
+  cudaStream_t stream = nullptr;
+  std::thread th;
+  std::mutex mu;
+  std::condition_variable cv;       // work arrived / stop
+  std::condition_variable done_cv;  // a request finished
+  std::deque<uint64_t> pending;
+  std::unordered_map<uint64_t, Request> reqs;
+  std::vector<int64_t> slot_ticket;
+  int active = 0;
+  bool stop = false;
+  uint64_t next_ticket = 1;
+  int64_t completed = 0;
+  int64_t levels = 0;
+  double busy_ms = 0;
+  int64_t state_bytes = 0;
+  bool wcc_ready = false;
+  std::string fatal;
+  DevBuf admit_dev, retire_dev, clear_dev, staging;
+  AdmitReq* h_admit = nullptr;
+  RetireReq* h_retire = nullptr;
+  uint64_t* h_clear = nullptr;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+
+  double now_ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  void loop();
+  void finish_wcc(std::vector<uint64_t>& tickets);
+  void retire(std::vector<int>& slots_to_retire, bool forced);
+};
+
+namespace {
+
+using AdmitFn = void (*)(const GroupDev&, const DevGraph&, const AdmitReq*, int, cudaStream_t);
+using RetireFn = void (*)(const GroupDev&, int64_t, const RetireReq*, int, uint32_t*,
+                          const uint64_t*, int, uint32_t, int, cudaStream_t);
+
+template <int W>
+AdmitFn admit_for(int ob) {
+  return ob == 8 ? launch_admit<W, int64_t> : launch_admit<W, int32_t>;
+}
+
+AdmitFn pick_admit(int W, int ob) {
+  switch (W) {
+    case 1: return admit_for<1>(ob);
+    case 2: return admit_for<2>(ob);
+    case 4: return admit_for<4>(ob);
+    case 8: return admit_for<8>(ob);
+    default: return admit_for<16>(ob);
+  }
+}
+
+RetireFn pick_retire(int W) {
+  switch (W) {
+    case 1: return launch_retire<1>;
+    case 2: return launch_retire<2>;
+    case 4: return launch_retire<4>;
+    case 8: return launch_retire<8>;
+    default: return launch_retire<16>;
+  }
+}
+
+GroupDev server_dev(cgp_server* sv) {
+  GroupDev g;
+  Workspace* ws = sv->ws.get();
+  g.visited = ws->visited.as<uint64_t>();
+  g.fbuf0 = ws->fbuf0.as<uint64_t>();
+  g.fbuf1 = ws->fbuf1.as<uint64_t>();
+  g.list0 = ws->list0.as<int32_t>();
+  g.list1 = ws->list1.as<int32_t>();
+  g.stamp = ws->stamp.as<int32_t>();
+  g.planes = nullptr;
+  g.values = ws->values.as<uint32_t>();
+  g.hacc = ws->hacc.as<uint64_t>();
+  g.ctl = ws->ctl.as<LevelCtl>();
+  g.prof = nullptr;
+  g.slots = ws->slots.as<SlotDev>();
+  g.Qg = sv->S;
+  return g;
+}
+
+}  // namespace
+
+void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
+  if (tickets.empty()) return;
+  if (!wcc_ready) {
+    ws->wcc.ensure(static_cast<size_t>(g->V) * 4);
+    wcc_labels(g, ws->wcc.as<uint32_t>(), stream);
+    wcc_ready = true;
+  }
+  std::vector<std::pair<void*, bool>> outs;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (uint64_t t : tickets) outs.emplace_back(reqs[t].out, reqs[t].out_dev);
+  }
+  for (auto& o : outs)
+    if (o.first)
+      ck(cudaMemcpyAsync(o.first, ws->wcc.p, static_cast<size_t>(g->V) * 4,
+                         o.second ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream),
+         "wcc result");
+  ck(cudaStreamSynchronize(stream), "wcc");
+  std::lock_guard<std::mutex> lk(mu);
+  const double t = now_ms();
+  for (uint64_t tk : tickets) {
+    Request& r = reqs[tk];
+    r.state = 2;
+    r.t_admit = r.t_admit > 0 ? r.t_admit : t;
+    r.t_finish = t;
+    r.completion_level = 0;
+    ++completed;
+  }
+  done_cv.notify_all();
+}
+
+void cgp_server::retire(std::vector<int>& to_retire, bool forced) {
+  const int64_t V = g->V;
+  const uint32_t f32 = g->weight_kind == CGP_WEIGHT_F32 ? 1u : 0u;
+  RetireFn rf = pick_retire(W);
+  for (size_t b = 0; b < to_retire.size(); b += kRetireBatch) {
+    const int n = static_cast<int>(std::min<size_t>(kRetireBatch, to_retire.size() - b));
+    std::memset(h_clear, 0, kMaxWords * 8);
+    std::vector<uint64_t> tickets(n);
+    std::vector<std::pair<void*, bool>> outs(n);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      for (int i = 0; i < n; ++i) {
+        const int s = to_retire[b + i];
+        tickets[i] = static_cast<uint64_t>(slot_ticket[s]);
+        Request& r = reqs[tickets[i]];
+        outs[i] = {r.out, r.out_dev};
+        h_retire[i].slot = s;
+        h_retire[i].kind = r.q.kind;
+        h_retire[i].has_out = (r.out != nullptr && !r.cancel) ? 1 : 0;
+        h_clear[s >> 6] |= 1ULL << (s & 63);
+      }
+    }
+    ck(cudaMemcpyAsync(retire_dev.p, h_retire, n * sizeof(RetireReq), cudaMemcpyHostToDevice, stream),
+       "upload retire");
+    ck(cudaMemcpyAsync(clear_dev.p, h_clear, kMaxWords * 8, cudaMemcpyHostToDevice, stream),
+       "upload clear");
+    rf(server_dev(this), V, retire_dev.as<RetireReq>(), n, staging.as<uint32_t>(),
+       clear_dev.as<uint64_t>(), forced ? 1 : 0, f32, g->num_sms * 8, stream);
+    ck(cudaGetLastError(), "retire");
+    for (int i = 0; i < n; ++i) {
+      if (h_retire[i].has_out)
+        ck(cudaMemcpyAsync(outs[i].first, staging.as<uint32_t>() + static_cast<size_t>(i) * V,
+                           static_cast<size_t>(V) * 4,
+                           outs[i].second ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                           stream),
+           "result copy");
+    }
+    ck(cudaStreamSynchronize(stream), "retire");
+    LevelCtl c;
+    ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
+    std::lock_guard<std::mutex> lk(mu);
+    const double t = now_ms();
+    for (int i = 0; i < n; ++i) {
+      Request& r = reqs[tickets[i]];
+      r.state = r.cancel ? 3 : 2;
+      r.t_finish = t;
+      r.completion_level = c.level - r.admit_level;
+      slot_ticket[h_retire[i].slot] = -1;
+      --active;
+      ++completed;
+    }
+    done_cv.notify_all();
+  }
+}
+
+void cgp_server::loop() {
+  try {
+    ck(cudaSetDevice(g->device), "cudaSetDevice");
+    AdmitFn af = pick_admit(W, g->offset_bytes);
+    const int per = o.levels_per_sync > 0 ? o.levels_per_sync : 2;
+    for (;;) {
+      std::vector<uint64_t> wcc_tickets;
+      int nadmit = 0;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait_for(lk, std::chrono::milliseconds(50),
+                    [&] { return stop || !pending.empty() || active > 0; });
+        if (stop) break;
+        const double t = now_ms();
+        while (!pending.empty()) {
+          const uint64_t tk = pending.front();
+          Request& r = reqs[tk];
+          if (r.cancel) {
+            pending.pop_front();
+            r.state = 3;
+            r.t_finish = t;
+            done_cv.notify_all();
+            continue;
+          }
+          if (r.q.kind == CGP_KIND_WCC) {
+            pending.pop_front();
+            r.state = 1;
+            r.t_admit = t;
+            wcc_tickets.push_back(tk);
+            continue;
+          }
+          int s = -1;
+          for (int i = 0; i < S; ++i)
+            if (slot_ticket[i] < 0) {
+              s = i;
+              break;
+            }
+          if (s < 0) break;
+          pending.pop_front();
+          slot_ticket[s] = static_cast<int64_t>(tk);
+          ++active;
+          r.state = 1;
+          r.slot = s;
+          r.t_admit = t;
+          h_admit[nadmit].slot = s;
+          h_admit[nadmit].kind = r.q.kind;
+          h_admit[nadmit].source = r.q.source;
+          h_admit[nadmit].k = r.q.k;
+          ++nadmit;
+        }
+      }
+      finish_wcc(wcc_tickets);
+      if (nadmit > 0) {
+        LevelCtl c;
+        ck(cudaMemcpyAsync(&c.level, reinterpret_cast<char*>(ws->ctl.p) + offsetof(LevelCtl, level),
+                           sizeof(int32_t), cudaMemcpyDeviceToHost, stream), "read level");
+        ck(cudaMemcpyAsync(admit_dev.p, h_admit, nadmit * sizeof(AdmitReq), cudaMemcpyHostToDevice,
+                           stream), "upload admits");
+        af(server_dev(this), g->dev_graph(), admit_dev.as<AdmitReq>(), nadmit, stream);
+        ck(cudaGetLastError(), "admit");
+        ck(cudaStreamSynchronize(stream), "admit");
+        std::lock_guard<std::mutex> lk(mu);
+        for (int i = 0; i < nadmit; ++i) reqs[slot_ticket[h_admit[i].slot]].admit_level = c.level;
+      }
+      int act;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        act = active;
+      }
+      if (act == 0) continue;
+      const double tb = now_ms();
+      GroupRun r;
+      group_enact(g, ws.get(), spec, o, stream, &r, per);
+      LevelCtl c;
+      ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
+      busy_ms += now_ms() - tb;
+      levels = c.level;
+      // converged: occupied, admitted before the current level, no frontier bit
+      std::vector<int> conv, forced;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        const uint64_t* act_bits = c.active[c.level & 1];
+        for (int s = 0; s < S; ++s) {
+          if (slot_ticket[s] < 0) continue;
+          Request& q = reqs[static_cast<uint64_t>(slot_ticket[s])];
+          const bool live = c.done != 1 && ((act_bits[s >> 6] >> (s & 63)) & 1ULL);
+          if (q.cancel) forced.push_back(s);
+          else if (q.admit_level < c.level && !live) conv.push_back(s);
+        }
+      }
+      if (!conv.empty()) retire(conv, false);
+      if (!forced.empty()) retire(forced, true);
+    }
+  } catch (...) {
+    cgp_status st = translate_exception();
+    char buf[512];
+    cgp_last_error(buf, sizeof(buf));
+    std::lock_guard<std::mutex> lk(mu);
+    fatal = std::string(cgp_status_name(st)) + ": " + buf;
+    for (auto& kv : reqs)
+      if (kv.second.state < 2) {
+        kv.second.state = 4;
+        kv.second.t_finish = now_ms();
+      }
+    done_cv.notify_all();
+  }
+}
+
+extern "C" {
+
+cgp_status cgp_server_create(cgp_graph* graph, int32_t slots, const cgp_options* opts,
+                             int64_t max_state_bytes, cgp_server** out) {
+  clear_error();
+  if (out == nullptr) return set_error(CGP_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (graph == nullptr) return set_error(CGP_ERR_INVALID_ARG, "graph is NULL");
+  if (slots <= 0 || slots > kMaxWords * 64)
+    return set_error(CGP_ERR_INVALID_ARG, "slots must be in [1, 1024]");
+  auto* sv = new (std::nothrow) cgp_server();
+  if (!sv) return set_error(CGP_ERR_OOM, "host allocation failed");
+  try {
+    GraphImpl* g = &graph->impl;
+    ck(cudaSetDevice(g->device), "cudaSetDevice");
+    sv->g = g;
+    if (opts) sv->o = *opts;
+    else cgp_options_init(&sv->o);
+    sv->o.profile_iterations = 0;
+    sv->o.max_iterations = 0;
+    // admission by device memory: slot width x |V| for the values, plus the
+    // per-vertex masks that every slot shares
+    size_t free_b = 0, total_b = 0;
+    ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const int64_t budget = max_state_bytes > 0 ? max_state_bytes
+                                               : static_cast<int64_t>(0.8 * static_cast<double>(free_b));
+    int S = slots;
+    while (S > 1 && group_state_bytes(g, choose_words(S, sv->o.mask_words), S, kDepthDirect) +
+                        static_cast<int64_t>(kRetireBatch) * g->V * 4 > budget)
+      --S;
+    const int64_t need = group_state_bytes(g, choose_words(S, sv->o.mask_words), S, kDepthDirect) +
+                         static_cast<int64_t>(kRetireBatch) * g->V * 4;
+    if (need > budget) throw ApiError{CGP_ERR_OOM, "not enough device memory for one slot"};
+    sv->S = S;
+    sv->W = choose_words(S, sv->o.mask_words);
+    sv->state_bytes = need;
+    sv->ws = std::make_unique<Workspace>(g->device);
+    sv->stream = sv->ws->stream;
+    sv->spec.W = sv->W;
+    sv->spec.Qg = S;
+    sv->spec.slots.assign(S, SlotDev{-1, -1, 0, 0});
+    sv->spec.depth_mode = kDepthDirect;
+    sv->spec.has_bfs = true;
+    sv->spec.has_sssp = true;
+    sv->spec.uniform_inf = kServeInf;
+    group_prepare(g, sv->ws.get(), sv->spec, sv->o, sv->stream);
+    sv->slot_ticket.assign(S, -1);
+    sv->admit_dev.ensure(kMaxWords * 64 * sizeof(AdmitReq));
+    sv->retire_dev.ensure(kRetireBatch * sizeof(RetireReq));
+    sv->clear_dev.ensure(kMaxWords * 8);
+    sv->staging.ensure(static_cast<size_t>(kRetireBatch) * g->V * 4);
+    ck(cudaHostAlloc(reinterpret_cast<void**>(&sv->h_admit), kMaxWords * 64 * sizeof(AdmitReq),
+                     cudaHostAllocDefault), "pinned");
+    ck(cudaHostAlloc(reinterpret_cast<void**>(&sv->h_retire), kRetireBatch * sizeof(RetireReq),
+                     cudaHostAllocDefault), "pinned");
+    ck(cudaHostAlloc(reinterpret_cast<void**>(&sv->h_clear), kMaxWords * 8, cudaHostAllocDefault),
+       "pinned");
+    ck(cudaStreamSynchronize(sv->stream), "server init");
+    sv->th = std::thread([sv] { sv->loop(); });
+    *out = sv;
+    return CGP_OK;
+  } catch (...) {
+    cgp_status st = translate_exception();
+    delete sv;
+    return st;
+  }
+}
+
+cgp_status cgp_server_destroy(cgp_server* sv) {
+  clear_error();
+  if (sv == nullptr) return CGP_OK;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv.notify_all();
+  if (sv->th.joinable()) sv->th.join();
+  if (sv->stream) cudaStreamSynchronize(sv->stream);
+  if (sv->h_admit) cudaFreeHost(sv->h_admit);
+  if (sv->h_retire) cudaFreeHost(sv->h_retire);
+  if (sv->h_clear) cudaFreeHost(sv->h_clear);
+  delete sv;
+  return CGP_OK;
+}
+
+cgp_status cgp_server_submit(cgp_server* sv, const cgp_query* q, void* out, int32_t out_on_device,
+                             uint64_t* ticket) {
+  clear_error();
+  if (sv == nullptr || q == nullptr || ticket == nullptr)
+    return set_error(CGP_ERR_INVALID_ARG, "NULL argument");
+  if (q->kind < CGP_KIND_BFS || q->kind > CGP_KIND_KHOP)
+    return set_error(CGP_ERR_INVALID_ARG, "unknown query kind");
+  if (q->kind != CGP_KIND_WCC && (q->source < 0 || q->source >= sv->g->V))
+    return set_error(CGP_ERR_INVALID_ARG, "query source out of range");
+  if (q->kind == CGP_KIND_KHOP && q->k < 0)
+    return set_error(CGP_ERR_INVALID_ARG, "k-hop bound must be non-negative");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  if (!sv->fatal.empty()) return set_error(CGP_ERR_CUDA, "server failed: " + sv->fatal);
+  const uint64_t t = sv->next_ticket++;
+  Request r;
+  r.q = *q;
+  r.out = out;
+  r.out_dev = out_on_device != 0;
+  r.t_submit = sv->now_ms();
+  sv->reqs.emplace(t, r);
+  sv->pending.push_back(t);
+  *ticket = t;
+  sv->cv.notify_all();
+  return CGP_OK;
+}
+
+static void fill_info(const Request& r, cgp_request_info* info) {
+  if (!info) return;
+  info->state = r.state;
+  info->slot = r.slot;
+  info->admit_level = r.admit_level;
+  info->completion_level = r.completion_level;
+  info->submit_time_ms = r.t_submit;
+  info->admit_time_ms = r.t_admit;
+  info->finish_time_ms = r.t_finish;
+}
+
+cgp_status cgp_server_poll(cgp_server* sv, uint64_t ticket, cgp_request_info* info) {
+  clear_error();
+  if (sv == nullptr) return set_error(CGP_ERR_INVALID_ARG, "server is NULL");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return set_error(CGP_ERR_NOT_FOUND, "unknown ticket");
+  fill_info(it->second, info);
+  return CGP_OK;
+}
+
+cgp_status cgp_server_wait(cgp_server* sv, uint64_t ticket, int32_t timeout_ms,
+                           cgp_request_info* info) {
+  clear_error();
+  if (sv == nullptr) return set_error(CGP_ERR_INVALID_ARG, "server is NULL");
+  std::unique_lock<std::mutex> lk(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return set_error(CGP_ERR_NOT_FOUND, "unknown ticket");
+  const auto pred = [&] { return sv->reqs[ticket].state >= 2; };
+  if (timeout_ms < 0) sv->done_cv.wait(lk, pred);
+  else if (!sv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred))
+    return set_error(CGP_ERR_TIMEOUT, "request not finished");
+  const Request& r = sv->reqs[ticket];
+  fill_info(r, info);
+  if (r.state == 3) return set_error(CGP_ERR_CANCELLED, "request cancelled");
+  if (r.state == 4) return set_error(CGP_ERR_CUDA, "server failed: " + sv->fatal);
+  return CGP_OK;
+}
+
+cgp_status cgp_server_cancel(cgp_server* sv, uint64_t ticket) {
+  clear_error();
+  if (sv == nullptr) return set_error(CGP_ERR_INVALID_ARG, "server is NULL");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  auto it = sv->reqs.find(ticket);
+  if (it == sv->reqs.end()) return set_error(CGP_ERR_NOT_FOUND, "unknown ticket");
+  if (it->second.state < 2) it->second.cancel = true;
+  sv->cv.notify_all();
+  return CGP_OK;
+}
+
+cgp_status cgp_server_drain(cgp_server* sv, int32_t timeout_ms) {
+  clear_error();
+  if (sv == nullptr) return set_error(CGP_ERR_INVALID_ARG, "server is NULL");
+  std::unique_lock<std::mutex> lk(sv->mu);
+  const auto pred = [&] {
+    if (!sv->fatal.empty()) return true;
+    for (auto& kv : sv->reqs)
+      if (kv.second.state < 2) return false;
+    return true;
+  };
+  if (timeout_ms < 0) sv->done_cv.wait(lk, pred);
+  else if (!sv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), pred))
+    return set_error(CGP_ERR_TIMEOUT, "requests still running");
+  if (!sv->fatal.empty()) return set_error(CGP_ERR_CUDA, "server failed: " + sv->fatal);
+  return CGP_OK;
+}
+
+cgp_status cgp_server_get_stats(cgp_server* sv, cgp_server_stats* st) {
+  clear_error();
+  if (sv == nullptr || st == nullptr) return set_error(CGP_ERR_INVALID_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(sv->mu);
+  st->slots = sv->S;
+  st->active_slots = sv->active;
+  st->queued = static_cast<int64_t>(sv->pending.size());
+  st->completed = sv->completed;
+  st->levels = sv->levels;
+  st->busy_ms = sv->busy_ms;
+  st->state_bytes = sv->state_bytes;
+  return CGP_OK;
+}
+
+}  // extern "C"

@@ -76,6 +76,7 @@ typedef int32_t cgp_status;
 
 typedef struct cgp_graph cgp_graph;
 typedef struct cgp_enactor cgp_enactor;
+typedef struct cgp_server cgp_server;
 
 /* query_descriptor_t (puercgp/include/puercgp/core/query_descriptor.hxx:19-24);
  * `k` is the hop bound of CGP_KIND_KHOP.  WCC ignores `source`. */
@@ -245,6 +246,53 @@ cgp_status cgp_enactor_frontier(cgp_enactor* e, int32_t* vertices,
 /* Writes the values of every query of the enactor (layout as cgp_batch_run). */
 cgp_status cgp_enactor_read_values(cgp_enactor* e, void* out, int32_t out_layout,
                                    int32_t out_on_device);
+
+/* --------------------------------------------------------------- serving --- */
+
+/* Continuous-batching server: replaces replenish_frontier_engine
+ * (puercgp/include/puercgp/engine/replenish_engine.hxx:42-554) and
+ * run_replenish_pipeline (replenish_engine.hxx:559-573).  Requests are
+ * admitted into free bitmask slots at level boundaries while others are in
+ * flight; state stays resident on the device; finished slots retire at level
+ * boundaries and are reused.  `slots` <= 1024.  max_state_bytes bounds the
+ * device memory the slot state may take (0 = 80% of free memory); the slot
+ * count is reduced to fit. */
+cgp_status cgp_server_create(cgp_graph* g, int32_t slots, const cgp_options* opts,
+                             int64_t max_state_bytes, cgp_server** out);
+cgp_status cgp_server_destroy(cgp_server* s);
+/* Queues a request.  out (nullable) receives V 4-byte values on completion;
+ * host memory unless out_on_device.  Returns a ticket. */
+cgp_status cgp_server_submit(cgp_server* s, const cgp_query* q, void* out,
+                             int32_t out_on_device, uint64_t* ticket);
+
+typedef struct {
+  int32_t state;             /* 0 queued, 1 running, 2 done, 3 cancelled, 4 failed */
+  int32_t slot;
+  int32_t admit_level;
+  int32_t completion_level;  /* query_result_t::completion_level (result.hxx:13-19) */
+  double submit_time_ms;     /* on the server's clock                               */
+  double admit_time_ms;
+  double finish_time_ms;     /* latency = finish - submit                           */
+} cgp_request_info;
+
+cgp_status cgp_server_poll(cgp_server* s, uint64_t ticket, cgp_request_info* info);
+/* Blocks until the ticket finishes or timeout_ms passes (CGP_ERR_TIMEOUT). */
+cgp_status cgp_server_wait(cgp_server* s, uint64_t ticket, int32_t timeout_ms,
+                           cgp_request_info* info);
+cgp_status cgp_server_cancel(cgp_server* s, uint64_t ticket);
+/* Blocks until every submitted request has finished (or timeout). */
+cgp_status cgp_server_drain(cgp_server* s, int32_t timeout_ms);
+
+typedef struct {
+  int32_t slots;
+  int32_t active_slots;
+  int64_t queued;
+  int64_t completed;
+  int64_t levels;
+  double busy_ms;
+  int64_t state_bytes;
+} cgp_server_stats;
+cgp_status cgp_server_get_stats(cgp_server* s, cgp_server_stats* st);
 
 /* ---------------------------------------------------- host-side inputs --- */
 

@@ -216,7 +216,10 @@ def _typed(kind, vec, graph):
         f = as_expected(vec, np.float32)
         if graph.weight_kind == 2:
             return f.view(np.uint32)
-        return np.where(np.isinf(f), 2**32 - 1, f).astype(np.uint32)
+        out = np.full(len(f), 2**32 - 1, np.uint32)
+        fin = np.isfinite(f)
+        out[fin] = f[fin].astype(np.uint32)
+        return out
     return np.asarray(vec, np.int64).astype(np.uint32)
 
 
