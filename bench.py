@@ -54,6 +54,11 @@ def parse_args():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--mode", default="hybrid")
     p.add_argument("--json-out", default="")
+    p.add_argument("--serve", action="store_true",
+                   help="serving workload: R-MAT 24, Poisson arrivals, p50/p99 latency")
+    p.add_argument("--serve-rates", default="500,2000,8000")
+    p.add_argument("--serve-seconds", type=float, default=3.0)
+    p.add_argument("--serve-slots", type=int, default=256)
     return p.parse_args()
 
 
@@ -236,11 +241,84 @@ def run_reference_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------ serving
+def serve_mix(g, n, seed, allowed=None):
+    """60% BFS, 30% SSSP, 10% k-hop BFS (k uniform in 2..6), sources uniform
+    over non-isolated vertices (seeded)."""
+    import cgp_b200 as cgp
+    rng = np.random.default_rng(seed)
+    src = g.pick_sources(n, seed=seed, allowed=allowed)
+    u = rng.random(n)
+    ks = rng.integers(2, 7, n)
+    out = []
+    for i in range(n):
+        kind = "bfs" if u[i] < 0.6 else ("sssp" if u[i] < 0.9 else "khop")
+        out.append(cgp.QueryDescriptor(int(src[i]), kind, int(ks[i]) if kind == "khop" else 0))
+    return out
+
+
+def poisson_run(server, descs, rate, seconds, seed):
+    """Submits requests at Poisson arrival times for `seconds`, waits for all,
+    returns latency percentiles and throughput."""
+    rng = np.random.default_rng(seed)
+    n = max(1, int(rate * seconds))
+    gaps = rng.exponential(1.0 / rate, n)
+    t_arr = np.cumsum(gaps)
+    tickets = []
+    t0 = time.perf_counter()
+    for i in range(n):
+        target = t0 + t_arr[i]
+        while True:
+            now = time.perf_counter()
+            if now >= target:
+                break
+            if target - now > 0.002:
+                time.sleep(target - now - 0.001)
+        tickets.append(server.submit(descs[i % len(descs)]))
+    server.drain()
+    infos = [server.wait(t) for t in tickets]
+    lat = np.array([i.latency_ms for i in infos])
+    done = [i for i in infos if i.state == "done"]
+    span = (max(i.finish_ms for i in done) - min(i.submit_ms for i in done)) / 1e3
+    return {"rate_qps": rate, "requests": n, "completed": len(done),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "throughput_qps": len(done) / span,
+            "sustained": bool(len(done) / span >= 0.9 * rate)}
+
+
+def run_serve(args):
+    import cgp_b200 as cgp
+    scale = args.scale if args.scale != 22 else 24
+    t = time.perf_counter()
+    g = cgp.gen_rmat(scale, args.edge_factor, 0.57, 0.19, 0.19, seed=1)
+    g = g.with_weights("u32", 1, 255, seed=2)
+    gen_s = time.perf_counter() - t
+    graph = cgp.CsrGraph(g, offsets64=True, symmetric=True)
+    descs = serve_mix(g, 4096, seed=42)
+    rows = []
+    with cgp.Server(graph, slots=args.serve_slots,
+                    options=cgp.RunOptions(traversal_mode=args.mode)) as srv:
+        poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
+        for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
+            rows.append(poisson_run(srv, descs, rate, args.serve_seconds, seed=100 + i))
+        st = srv.stats()
+    line = {"metric": "serve p50/p99 latency", "unit": "ms", "workload":
+            f"rmat{scale}_serving_mix60_30_10", "V": g.num_vertices, "E": g.num_edges,
+            "offsets": "int64", "slots": st["slots"], "state_bytes": st["state_bytes"],
+            "seconds_per_rate": args.serve_seconds, "rates": rows, "graph_gen_s": gen_s}
+    print(json.dumps(line), flush=True)
+    if args.json_out:
+        Path(args.json_out).write_text(json.dumps(line) + "\n")
+    return 0
+
+
 # ------------------------------------------------------------------ GPU arm
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.serve:
+        return run_serve(args)
     import torch
     import torch.distributed as dist
     import cgp_b200 as cgp
@@ -399,6 +477,17 @@ def main():
                "steps": args.e2e_steps, "ms_per_step": 1e3 * t_e2e / args.e2e_steps,
                "output": "pinned host buffers, vertex-major int32/uint32"}
 
+    # ---- serving: continuous batching on the same graph, Poisson arrivals
+    serving = None
+    if rank == 0 and args.serve_seconds > 0:
+        mix = serve_mix(g, 2048, seed=43, allowed=allowed.astype(np.uint8))
+        with cgp.Server(graph, slots=args.serve_slots,
+                        options=cgp.RunOptions(traversal_mode=args.mode)) as srv:
+            poisson_run(srv, mix[:64], 200, 0.3, seed=7)
+            serving = poisson_run(srv, mix, 2000.0, args.serve_seconds, seed=8)
+            serving["slots"] = srv.stats()["slots"]
+            serving["mix"] = "60% BFS / 30% SSSP / 10% k-hop (k in 2..6)"
+
     # ---- CPU baseline (rank 0, N = 1): the reference CPU traversal, bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -408,7 +497,12 @@ def main():
         dt, edges, kind, (cb, cs) = cpu_reference_sample(g, bfs_src[:nb], sssp_src[:ns], threads)
         hb_all = out_b[:, :nb].cpu().numpy().T
         hs_all = out_s[:, :ns].cpu().numpy().T.view(np.uint32)
-        cs_u = np.where(np.isinf(cs), 2**32 - 1, cs).astype(np.uint32) if cs.dtype == np.float32 else cs
+        if cs.dtype == np.float32:  # the reference's float distances -> uint32 words
+            cs_u = np.full(cs.shape, 2**32 - 1, np.uint32)
+            fin = np.isfinite(cs)
+            cs_u[fin] = cs[fin].astype(np.uint32)
+        else:
+            cs_u = cs
         cpu = {"value": edges / dt / 1e9, "unit": "GTEPS", "cores": threads, "kind": kind,
                "sample": f"{nb} BFS + {ns} SSSP queries of the workload, one query per thread "
                          f"({dt:.1f} s)",
@@ -442,6 +536,7 @@ def main():
             "one_query": one_query,
             "batched_vs_one_query": (value / world / one_query["gteps"]) if one_query else None,
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+            "serving": serving,
             "cpu_baseline": cpu, "graph_gen_s": gen_s,
         }
         s = json.dumps(line)
