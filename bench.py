@@ -360,9 +360,11 @@ def main():
     stream = torch.cuda.current_stream(dev)
     opts = cgp.RunOptions(traversal_mode=args.mode, stream=stream.cuda_stream)
 
+    empty = cgp.RunResult(values=None, iterations=0, gpu_time_ms=0.0, wall_time_ms=0.0)
+
     def step():
-        rb = cgp.run_batch(graph, bfs_d, opts, out=out_b)
-        rs = cgp.run_batch(graph, sssp_d, opts, out=out_s)
+        rb = cgp.run_batch(graph, bfs_d, opts, out=out_b) if bfs_d else empty
+        rs = cgp.run_batch(graph, sssp_d, opts, out=out_s) if sssp_d else empty
         return rb, rs
 
     for _ in range(max(3, args.warmup)):
@@ -401,9 +403,9 @@ def main():
     # ---- profiled step: per-kernel-class CUDA-event times + level counters
     popts = cgp.RunOptions(traversal_mode=args.mode, stream=stream.cuda_stream,
                            profile_kernels=True, profile_iterations=True)
-    pb = cgp.run_batch(graph, bfs_d, popts, out=out_b)
-    ps = cgp.run_batch(graph, sssp_d, popts, out=out_s)
-    W = pb.mask_words
+    pb = cgp.run_batch(graph, bfs_d, popts, out=out_b) if bfs_d else empty
+    ps = cgp.run_batch(graph, sssp_d, popts, out=out_s) if sssp_d else empty
+    W = pb.mask_words or ps.mask_words
     bytes_b = level_bytes(pb.iteration_profiles, "bfs", V, W)
     bytes_s = level_bytes(ps.iteration_profiles, "sssp", V, ps.mask_words)
     kclass = {}
@@ -430,7 +432,7 @@ def main():
 
     # ---- one-query form: the same kernels with Q = 1, back to back
     one_query = None
-    if not args.no_one_query and rank == 0:
+    if not args.no_one_query and rank == 0 and bfs_d and sssp_d:
         nb1, ns1 = min(16, len(bfs_d)), min(8, len(sssp_d))
         o1 = torch.empty((V, 1), dtype=torch.int32, device=dev)
         for d in (bfs_d[0], sssp_d[0]):
@@ -461,13 +463,16 @@ def main():
         hb = torch.empty((V, len(bfs_d)), dtype=torch.int32, pin_memory=True)
         hs = torch.empty((V, len(sssp_d)), dtype=torch.int32, pin_memory=True)
         eopts = cgp.RunOptions(traversal_mode=args.mode)
-        cgp.run_batch(graph, bfs_d, eopts, out=hb)
-        cgp.run_batch(graph, sssp_d, eopts, out=hs)
+        def e2e_step():
+            if bfs_d:
+                cgp.run_batch(graph, bfs_d, eopts, out=hb)
+            if sssp_d:
+                cgp.run_batch(graph, sssp_d, eopts, out=hs)
+        e2e_step()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            cgp.run_batch(graph, bfs_d, eopts, out=hb)
-            cgp.run_batch(graph, sssp_d, eopts, out=hs)
+            e2e_step()
         t_e2e = time.perf_counter() - t0
         t_e2e = allreduce(t_e2e, dist.ReduceOp.MAX if world > 1 else None)
         e_edges = allreduce(edges_step * args.e2e_steps, dist.ReduceOp.SUM if world > 1 else None)
@@ -490,7 +495,7 @@ def main():
 
     # ---- CPU baseline (rank 0, N = 1): the reference CPU traversal, bounded sample
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and bfs_d and sssp_d:
         threads = os.cpu_count() or 1
         nb = min(len(bfs_d), max(1, threads))
         ns = min(len(sssp_d), max(1, threads // 2))
@@ -527,11 +532,11 @@ def main():
                        "parallelism": f"query-sharded x{world}"},
             "queries_per_s": qps,
             "bfs": {"ms": t_b / args.steps,
-                    "gteps": comp_edges * len(bfs_d) / (t_b / args.steps / 1e3) / 1e9,
+                    "gteps": comp_edges * len(bfs_d) / max(t_b / args.steps / 1e3, 1e-12) / 1e9,
                     "iterations": rb.iterations, "push_levels": rb.push_levels,
                     "pull_levels": rb.pull_levels},
             "sssp": {"ms": t_s / args.steps,
-                     "gteps": comp_edges * len(sssp_d) / (t_s / args.steps / 1e3) / 1e9,
+                     "gteps": comp_edges * len(sssp_d) / max(t_s / args.steps / 1e3, 1e-12) / 1e9,
                      "iterations": rs.iterations},
             "one_query": one_query,
             "batched_vs_one_query": (value / world / one_query["gteps"]) if one_query else None,
