@@ -247,6 +247,37 @@ cgp_status cgp_enactor_frontier(cgp_enactor* e, int32_t* vertices,
 cgp_status cgp_enactor_read_values(cgp_enactor* e, void* out, int32_t out_layout,
                                    int32_t out_on_device);
 
+/* ------------------------------------------------- allocation-free BFS --- */
+
+/* Size of the fixed device array that cgp_bfs_batch_noalloc works in (held by
+ * every GPU that loads the library until the process exits), and its query
+ * limit. */
+#define CGP_NOALLOC_SCRATCH_BYTES (24u << 20)
+#define CGP_NOALLOC_MAX_QUERIES 256
+
+/* Batched BFS that allocates no memory.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc where they need a traversal (a
+ * framework that reserved the device memory pool up front, latency paths
+ * where cudaMalloc/cudaFree would synchronise the device, hosts that only
+ * lend their own buffers).  The caller passes a device CSR (row_offsets of
+ * offset_bytes 4 or 8, num_vertices + 1 entries; col_indices, num_edges
+ * entries), host `sources` (nq <= 256) and a device output of
+ * num_vertices * nq int32 depths, vertex-major out[v*nq + q], INT32_MAX for
+ * unreached.  Working state lives in one static device array of
+ * CGP_NOALLOC_SCRATCH_BYTES: about 36*V bytes for up to 64 queries and
+ * 108*V bytes for up to 256, plus 8 KiB; larger graphs are rejected with
+ * CGP_ERR_INVALID_ARG.  symmetric != 0 (the CSR holds both directions)
+ * allows pull levels; otherwise every level pushes.  The work is enqueued on
+ * `stream` (cudaStream_t, NULL = default stream) of the current device and
+ * the call returns when it is done.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Calls share the array: calls that overlap on the same device race and must
+ * be serialised by the caller. */
+cgp_status cgp_bfs_batch_noalloc(const void* row_offsets, int32_t offset_bytes,
+                                 const int32_t* col_indices, int64_t num_vertices,
+                                 int64_t num_edges, const int32_t* sources, int32_t nq,
+                                 int32_t symmetric, int32_t* out, void* stream);
+
 /* --------------------------------------------------------------- serving --- */
 
 /* Continuous-batching server: replaces replenish_frontier_engine
