@@ -53,6 +53,9 @@ def parse_args():
     p.add_argument("--no-one-query", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--mode", default="hybrid")
+    p.add_argument("--pull-edge-ratio", type=float, default=0.20)
+    p.add_argument("--pull-frontier-ratio", type=float, default=0.15)
+    p.add_argument("--heavy-degree", type=int, default=0)
     p.add_argument("--json-out", default="")
     p.add_argument("--serve", action="store_true",
                    help="serving workload: R-MAT 24, Poisson arrivals, p50/p99 latency")
@@ -358,7 +361,9 @@ def main():
     out_b = torch.empty((V, len(bfs_d)), dtype=torch.int32, device=dev)
     out_s = torch.empty((V, len(sssp_d)), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
-    opts = cgp.RunOptions(traversal_mode=args.mode, stream=stream.cuda_stream)
+    tuning = dict(traversal_mode=args.mode, pull_edge_ratio=args.pull_edge_ratio,
+                  pull_frontier_ratio=args.pull_frontier_ratio, heavy_degree=args.heavy_degree)
+    opts = cgp.RunOptions(stream=stream.cuda_stream, **tuning)
 
     empty = cgp.RunResult(values=None, iterations=0, gpu_time_ms=0.0, wall_time_ms=0.0)
 
@@ -401,8 +406,8 @@ def main():
     qps = (len(bfs_d) + len(sssp_d)) * args.steps * world / (ms_max / 1e3)
 
     # ---- profiled step: per-kernel-class CUDA-event times + level counters
-    popts = cgp.RunOptions(traversal_mode=args.mode, stream=stream.cuda_stream,
-                           profile_kernels=True, profile_iterations=True)
+    popts = cgp.RunOptions(stream=stream.cuda_stream, profile_kernels=True,
+                           profile_iterations=True, **tuning)
     pb = cgp.run_batch(graph, bfs_d, popts, out=out_b) if bfs_d else empty
     ps = cgp.run_batch(graph, sssp_d, popts, out=out_s) if sssp_d else empty
     W = pb.mask_words or ps.mask_words
@@ -462,7 +467,7 @@ def main():
     if args.e2e_steps > 0:
         hb = torch.empty((V, len(bfs_d)), dtype=torch.int32, pin_memory=True)
         hs = torch.empty((V, len(sssp_d)), dtype=torch.int32, pin_memory=True)
-        eopts = cgp.RunOptions(traversal_mode=args.mode)
+        eopts = cgp.RunOptions(**tuning)
         def e2e_step():
             if bfs_d:
                 cgp.run_batch(graph, bfs_d, eopts, out=hb)
@@ -525,7 +530,8 @@ def main():
                        "V": V, "E": g.num_edges, "weights": "u32 uniform [1,64]",
                        "queries_per_gpu": {"bfs": len(bfs_d), "sssp": len(sssp_d)},
                        "mask_words": W, "largest_component_vertices": comp_v,
-                       "traversal_mode": args.mode,
+                       "traversal_mode": args.mode, "pull_edge_ratio": args.pull_edge_ratio,
+                       "pull_frontier_ratio": args.pull_frontier_ratio,
                        "l2": f"inputs larger than L2: CSR {4 * (V + 1 + 2 * g.num_edges) / 2**20:.0f} MiB "
                              f"+ outputs {8 * V * (len(bfs_d) + len(sssp_d)) / 2**30:.1f} GiB "
                              f"per step, re-initialised every step (no flush)",

@@ -609,19 +609,19 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
 void group_write_output(GraphImpl* g, Workspace* ws, GroupSpec& spec, OutMap om,
                         int query_major, cudaStream_t s) {
   spec.launches++;
-  const int blocks = g->num_sms * 16;
+  const dim3 grid(g->num_sms * 8, query_major ? std::min(spec.Qg, 65535) : 1);
   if (spec.depth_mode == kDepthPlanes) {
     LevelCtl c;
     ck(cudaMemcpyAsync(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost, s), "read ctl");
     ck(cudaStreamSynchronize(s), "read ctl");
     switch (spec.W) {
-#define CGP_MAT(WW) case WW: k_materialize_planes<WW><<<blocks, kBlock, 0, s>>>(ws->visited.as<uint64_t>(), ws->planes.as<uint64_t>(), c.num_planes, g->V, spec.Qg, om, query_major); break;
+#define CGP_MAT(WW) case WW: k_materialize_planes<WW><<<grid, kBlock, 0, s>>>(ws->visited.as<uint64_t>(), ws->planes.as<uint64_t>(), c.num_planes, g->V, spec.Qg, om, query_major); break;
       CGP_MAT(1) CGP_MAT(2) CGP_MAT(4) CGP_MAT(8) CGP_MAT(16)
 #undef CGP_MAT
     }
   } else {
-    k_copy_values<<<blocks, kBlock, 0, s>>>(ws->values.as<uint32_t>(), ws->slots.as<SlotDev>(),
-                                            g->V, spec.Qg, om, query_major);
+    k_copy_values<<<grid, kBlock, 0, s>>>(group_dev(ws, spec, false).values, ws->slots.as<SlotDev>(),
+                                          g->V, spec.Qg, om, query_major);
   }
   ck(cudaGetLastError(), "write output");
 }

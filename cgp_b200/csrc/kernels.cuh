@@ -721,6 +721,93 @@ __device__ __forceinline__ bool sssp_relax(const GroupDev& g, const LevelView& l
   return atomicMax(g.stamp + n, lv.level + 1) < lv.level + 1;
 }
 
+// Relaxation with the weight already loaded (raw 32-bit pattern).
+template <int WK>
+__device__ __forceinline__ uint32_t relax_w(uint32_t du, uint32_t wbits) {
+  if constexpr (WK == kWeightF32) {
+    return __float_as_uint(__fadd_rn(__uint_as_float(du), __uint_as_float(wbits)));
+  } else {
+    const uint32_t wt = (WK == kWeightU32) ? wbits : 1u;
+    return du > 0xffffffffu - wt ? 0xffffffffu : du + wt;
+  }
+}
+
+template <int WK>
+__device__ __forceinline__ uint32_t weight_bits(const void* w, int64_t e) {
+  if constexpr (WK == kWeightNone) {
+    return 1u;
+  } else {
+    return static_cast<const uint32_t*>(w)[e];
+  }
+}
+
+// Vertices with more active SSSP bits than this take the dense path.
+constexpr int kDenseBits = 16;
+
+// Dense SSSP relaxation of edges [eb, ee) of vertex u by one warp (all lanes
+// call).  Lane j owns query 32c+j of every 32-bit chunk c of the vertex's
+// active mask: u's distances stay in registers, and per edge each active
+// chunk costs one coalesced 128-byte load of the neighbour's row, a compare,
+// and an atomicMin only where it improves; the improved bits of a chunk are
+// combined by a ballot into one atomicOr of the next-frontier word.
+template <int W, typename OT, int WK>
+__device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGraph& G,
+                                                 const LevelView& lv, int32_t u,
+                                                 const uint64_t (&bits)[W], int64_t eb,
+                                                 int64_t ee, int lane, uint64_t (&uni)[W],
+                                                 unsigned long long& improved) {
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  uint32_t half[2 * W];
+  uint32_t du[2 * W];
+#pragma unroll
+  for (int c = 0; c < 2 * W; ++c) {
+    half[c] = static_cast<uint32_t>(bits[c >> 1] >> (32 * (c & 1)));
+    du[c] = ((half[c] >> lane) & 1u)
+                ? g.values[static_cast<size_t>(u) * Qg + 32 * c + lane]
+                : 0xffffffffu;
+  }
+  for (int64_t e0 = eb; e0 < ee; e0 += 32) {
+    const int64_t e = e0 + lane;
+    int32_t nl = 0;
+    uint32_t wl = 0;
+    if (e < ee) {
+      nl = G.col[e];
+      wl = weight_bits<WK>(G.w, e);
+    }
+    const int cnt = static_cast<int>(ee - e0 < 32 ? ee - e0 : 32);
+    for (int i = 0; i < cnt; ++i) {
+      const int32_t nb = __shfl_sync(kFull, nl, i);
+      const uint32_t wt = __shfl_sync(kFull, wl, i);
+      uint32_t* row = g.values + static_cast<size_t>(nb) * Qg;
+      bool any = false;
+#pragma unroll
+      for (int c = 0; c < 2 * W; ++c) {
+        if (half[c] == 0) continue;
+        bool imp = false;
+        if ((half[c] >> lane) & 1u) {
+          const uint32_t cand = relax_w<WK>(du[c], wt);
+          uint32_t* dst = row + 32 * c + lane;
+          if (cand < *dst) imp = cand < atomicMin(dst, cand);
+        }
+        const unsigned m = __ballot_sync(kFull, imp);
+        if (m) {
+          any = true;
+          if (lane == 0) {
+            const uint64_t bitsw = static_cast<uint64_t>(m) << (32 * (c & 1));
+            atomic_or64(lv.fnext + static_cast<size_t>(nb) * W + (c >> 1), bitsw);
+            uni[c >> 1] |= bitsw;
+            improved += __popc(m);
+          }
+        }
+      }
+      bool app = false;
+      if (any && lane == 0) app = atomicMax(g.stamp + nb, lv.level + 1) < lv.level + 1;
+      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist, lv.ncount, lv.nedges,
+                  lane);
+    }
+  }
+}
+
 // SSSP push over the frontier list: the (edge, active query) pairs of a tile
 // of 32 vertices are flattened and spread evenly over the warp's lanes, so a
 // vertex with k active queries and degree d costs k*d/32 warp steps.
@@ -768,9 +855,23 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
     }
     const int64_t deg = end - beg;
     const bool work = valid && k > 0 && deg > 0 && deg <= G.heavy_degree;
-    long long wk = work ? static_cast<long long>(k) * deg : 0;
-    spairs += static_cast<unsigned long long>(wk);
+    spairs += work ? static_cast<unsigned long long>(k) * static_cast<unsigned long long>(deg) : 0ULL;
     sactive += static_cast<unsigned long long>(k);
+    // vertices with many active queries: the whole warp, one at a time
+    unsigned dense = __ballot_sync(kFull, work && k > kDenseBits);
+    while (dense) {
+      const int src = __ffs(dense) - 1;
+      dense &= dense - 1;
+      const int32_t bu = __shfl_sync(kFull, u, src);
+      const int64_t bb = __shfl_sync(kFull, beg, src);
+      const int64_t be = __shfl_sync(kFull, end, src);
+      uint64_t bbits[W];
+#pragma unroll
+      for (int i = 0; i < W; ++i) bbits[i] = __shfl_sync(kFull, b[i], src);
+      sssp_dense_edges<W, OT, WK>(g, G, lv, bu, bbits, bb, be, lane, uni, improved);
+    }
+    // the rest: (edge, query) pairs flattened over the lanes
+    long long wk = (work && k <= kDenseBits) ? static_cast<long long>(k) * deg : 0;
     long long inc = wk;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -798,10 +899,10 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
           else lo = mid + 1;
         }
         const long long start = lo ? s_inc[wib][lo - 1] : 0;
-        const long long local = p - start;
+        const int local = static_cast<int>(p - start);  // < kDenseBits * heavy_degree
         const int ko = s_k[wib][lo];
-        const long long eoff = local / ko;
-        const int j = static_cast<int>(local - eoff * ko);
+        const int eoff = local / ko;
+        const int j = local - eoff * ko;
         const int q = jth_set_bit<W>(s_b[wib][lo], j);
         const int64_t e = s_beg[wib][lo] + eoff;
         nb = G.col[e];
@@ -866,6 +967,24 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
       __syncthreads();
       continue;
     }
+    if (k > kDenseBits) {
+      // each warp takes a contiguous slice of the chunk's edges
+      const int64_t beg = row_at<OT>(G.row, u);
+      const int64_t end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
+      const int64_t cb = beg + (c - G.heavy_chunk_start[h]) * kHeavyChunk;
+      const int64_t ce = min(end, cb + kHeavyChunk);
+      if (threadIdx.x == 0) {
+        atomicAdd(&g.ctl->lc.sssp_pairs, static_cast<unsigned long long>(ce - cb) * k);
+        if (c == G.heavy_chunk_start[h]) atomicAdd(&g.ctl->lc.sssp_active, static_cast<unsigned long long>(k));
+      }
+      const int nw = blockDim.x >> 5;
+      const int64_t seg = (ce - cb + nw - 1) / nw;
+      const int64_t wb = cb + (threadIdx.x >> 5) * seg;
+      const int64_t we = min(ce, wb + seg);
+      sssp_dense_edges<W, OT, WK>(g, G, lv, u, b, wb, we, lane, uni, improved);
+      __syncthreads();
+      continue;
+    }
     for (int t = threadIdx.x; t < W * 64; t += blockDim.x) {
       const int i = t >> 6, bit = t & 63;
       if ((b[i] >> bit) & 1ULL)
@@ -886,8 +1005,8 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
       int32_t nb = 0;
       bool app = false;
       if (p < pairs) {
-        const long long eoff = p / k;
-        const int q = s_q[p - eoff * k];
+        const int eoff = static_cast<int>(p) / k;  // pairs <= kHeavyChunk * kDenseBits
+        const int q = s_q[static_cast<int>(p) - eoff * k];
         const int64_t e = cb + eoff;
         nb = G.col[e];
         app = sssp_relax<W, WK>(g, lv, u, nb, q, G.w, e, uni, improved);
@@ -1029,70 +1148,86 @@ __global__ void k_seed(GroupDev g, DevGraph G) {
 // --------------------------------------------------------------- output
 // Fills the working values with each slot's "unreached" marker, or with
 // `uniform` everywhere when it is nonzero (the serving layout, where a slot
-// changes kind between requests).
+// changes kind between requests).  Warp per vertex row, lanes over slots.
 static __global__ void k_fill_values(uint32_t* values, const SlotDev* slots, int Qg,
-                              int64_t V, uint32_t f32_inf_for_sssp, uint32_t uniform) {
-  const size_t total = static_cast<size_t>(V) * Qg;
-  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    if (uniform) {
-      values[i] = uniform;
-      continue;
+                                     int64_t V, uint32_t f32_inf_for_sssp, uint32_t uniform) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t v = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < V;
+       v += warps) {
+    uint32_t* row = values + static_cast<size_t>(v) * Qg;
+    for (int q = lane; q < Qg; q += 32) {
+      uint32_t x = uniform;
+      if (!uniform) {
+        const int kind = slots[q].kind;
+        x = kind == 1 ? f32_inf_for_sssp : (kind == 2 ? 0u : 0x7fffffffu);
+      }
+      row[q] = x;
     }
-    const int q = static_cast<int>(i % Qg);
-    const int kind = slots[q].kind;
-    values[i] = kind == 1 ? f32_inf_for_sssp : (kind == 2 ? 0u : 0x7fffffffu);
   }
 }
 
-
 // Depth planes -> int32 depths (INT32_MAX where the visited bit is clear).
-// Thread per (vertex, query); consecutive threads walk the contiguous axis.
+// Vertex-major output: warp per vertex, lanes over queries (coalesced row
+// writes).  Query-major output: blockIdx.y walks queries, threads walk
+// vertices (coalesced column writes).
+template <int W>
+__device__ __forceinline__ uint32_t plane_depth(const uint64_t* visited, const uint64_t* planes,
+                                                int K, int64_t V, int64_t v, int q) {
+  const size_t word = static_cast<size_t>(v) * W + (q >> 6);
+  const uint64_t bit = 1ULL << (q & 63);
+  if (!(visited[word] & bit)) return 0x7fffffffu;
+  uint32_t d = 0;
+  for (int b = 0; b < K; ++b)
+    if (planes[static_cast<size_t>(b) * V * W + word] & bit) d |= 1u << b;
+  return d;
+}
+
 template <int W>
 __global__ void k_materialize_planes(const uint64_t* visited, const uint64_t* planes,
                                      int K, int64_t V, int Qg, OutMap om, int query_major) {
-  const size_t total = static_cast<size_t>(V) * Qg;
-  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    int64_t v;
-    int q;
-    if (query_major) {
-      q = static_cast<int>(i / V);
-      v = static_cast<int64_t>(i % V);
-    } else {
-      v = static_cast<int64_t>(i / Qg);
-      q = static_cast<int>(i % Qg);
+  if (query_major) {
+    for (int q = blockIdx.y; q < Qg; q += gridDim.y) {
+      uint32_t* col = om.out + static_cast<int64_t>(om.qmap[q]) * om.sq;
+      for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
+           v += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        col[v * om.sv] = plane_depth<W>(visited, planes, K, V, v, q);
     }
-    const size_t word = static_cast<size_t>(v) * W + (q >> 6);
-    const uint64_t bit = 1ULL << (q & 63);
-    uint32_t d = 0x7fffffffu;
-    if (visited[word] & bit) {
-      d = 0;
-      for (int b = 0; b < K; ++b)
-        if (planes[static_cast<size_t>(b) * V * W + word] & bit) d |= 1u << b;
-    }
-    om.out[v * om.sv + static_cast<int64_t>(om.qmap[q]) * om.sq] = d;
+    return;
+  }
+  if (blockIdx.y != 0) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t v = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < V;
+       v += warps) {
+    uint32_t* row = om.out + v * om.sv;
+    for (int q = lane; q < Qg; q += 32)
+      row[static_cast<int64_t>(om.qmap[q]) * om.sq] = plane_depth<W>(visited, planes, K, V, v, q);
   }
 }
 
-// Working values -> output mapping (skips WCC slots).
+// Working values -> output mapping (skips WCC slots); same mappings.
 static __global__ void k_copy_values(const uint32_t* values, const SlotDev* slots, int64_t V,
-                              int Qg, OutMap om, int query_major) {
-  const size_t total = static_cast<size_t>(V) * Qg;
-  for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    int64_t v;
-    int q;
-    if (query_major) {
-      q = static_cast<int>(i / V);
-      v = static_cast<int64_t>(i % V);
-    } else {
-      v = static_cast<int64_t>(i / Qg);
-      q = static_cast<int>(i % Qg);
+                                     int Qg, OutMap om, int query_major) {
+  if (query_major) {
+    for (int q = blockIdx.y; q < Qg; q += gridDim.y) {
+      if (slots[q].kind == 2) continue;
+      uint32_t* col = om.out + static_cast<int64_t>(om.qmap[q]) * om.sq;
+      for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
+           v += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        col[v * om.sv] = values[static_cast<size_t>(v) * Qg + q];
     }
-    if (slots[q].kind == 2) continue;
-    om.out[v * om.sv + static_cast<int64_t>(om.qmap[q]) * om.sq] =
-        values[static_cast<size_t>(v) * Qg + q];
+    return;
+  }
+  if (blockIdx.y != 0) return;
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t v = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < V;
+       v += warps) {
+    const uint32_t* src = values + static_cast<size_t>(v) * Qg;
+    uint32_t* row = om.out + v * om.sv;
+    for (int q = lane; q < Qg; q += 32)
+      if (slots[q].kind != 2) row[static_cast<int64_t>(om.qmap[q]) * om.sq] = src[q];
   }
 }
 
