@@ -22,6 +22,7 @@ host cores instead.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -56,6 +57,7 @@ def parse_args():
     p.add_argument("--pull-edge-ratio", type=float, default=0.20)
     p.add_argument("--pull-frontier-ratio", type=float, default=0.15)
     p.add_argument("--heavy-degree", type=int, default=0)
+    p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--json-out", default="")
     p.add_argument("--serve", action="store_true",
                    help="serving workload: R-MAT 24, Poisson arrivals, p50/p99 latency")
@@ -303,7 +305,15 @@ def run_serve(args):
                     options=cgp.RunOptions(traversal_mode=args.mode)) as srv:
         poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
-            rows.append(poisson_run(srv, descs, rate, args.serve_seconds, seed=100 + i))
+            s0 = srv.stats()
+            row = poisson_run(srv, descs, rate, args.serve_seconds, seed=100 + i)
+            s1 = srv.stats()
+            row["levels"] = s1["levels"] - s0["levels"]
+            row["level_ms"] = (s1["busy_ms"] - s0["busy_ms"]) / max(1, row["levels"])
+            row["retire_ms"] = s1["retire_ms"] - s0["retire_ms"]
+            row["retire_passes"] = s1["retire_passes"] - s0["retire_passes"]
+            row["admit_ms"] = s1["admit_ms"] - s0["admit_ms"]
+            rows.append(row)
         st = srv.stats()
     line = {"metric": "serve p50/p99 latency", "unit": "ms", "workload":
             f"rmat{scale}_serving_mix60_30_10", "V": g.num_vertices, "E": g.num_edges,
@@ -366,10 +376,19 @@ def main():
     opts = cgp.RunOptions(stream=stream.cuda_stream, **tuning)
 
     empty = cgp.RunResult(values=None, iterations=0, gpu_time_ms=0.0, wall_time_ms=0.0)
+    # autotuner (untimed): mask width, heavy threshold, pull threshold per batch
+    opts_b = opts_s = opts
+    tune_s = time.perf_counter()
+    if not args.no_autotune:
+        if bfs_d:
+            opts_b = cgp.autotune(graph, bfs_d, opts, reps=2)
+        if sssp_d:
+            opts_s = cgp.autotune(graph, sssp_d, opts, reps=2)
+    tune_s = time.perf_counter() - tune_s
 
     def step():
-        rb = cgp.run_batch(graph, bfs_d, opts, out=out_b) if bfs_d else empty
-        rs = cgp.run_batch(graph, sssp_d, opts, out=out_s) if sssp_d else empty
+        rb = cgp.run_batch(graph, bfs_d, opts_b, out=out_b) if bfs_d else empty
+        rs = cgp.run_batch(graph, sssp_d, opts_s, out=out_s) if sssp_d else empty
         return rb, rs
 
     for _ in range(max(3, args.warmup)):
@@ -406,10 +425,12 @@ def main():
     qps = (len(bfs_d) + len(sssp_d)) * args.steps * world / (ms_max / 1e3)
 
     # ---- profiled step: per-kernel-class CUDA-event times + level counters
-    popts = cgp.RunOptions(stream=stream.cuda_stream, profile_kernels=True,
-                           profile_iterations=True, **tuning)
-    pb = cgp.run_batch(graph, bfs_d, popts, out=out_b) if bfs_d else empty
-    ps = cgp.run_batch(graph, sssp_d, popts, out=out_s) if sssp_d else empty
+    pb = (cgp.run_batch(graph, bfs_d, dataclasses.replace(opts_b, profile_kernels=True,
+                                                          profile_iterations=True), out=out_b)
+          if bfs_d else empty)
+    ps = (cgp.run_batch(graph, sssp_d, dataclasses.replace(opts_s, profile_kernels=True,
+                                                           profile_iterations=True), out=out_s)
+          if sssp_d else empty)
     W = pb.mask_words or ps.mask_words
     bytes_b = level_bytes(pb.iteration_profiles, "bfs", V, W)
     bytes_s = level_bytes(ps.iteration_profiles, "sssp", V, ps.mask_words)
@@ -440,20 +461,22 @@ def main():
     if not args.no_one_query and rank == 0 and bfs_d and sssp_d:
         nb1, ns1 = min(16, len(bfs_d)), min(8, len(sssp_d))
         o1 = torch.empty((V, 1), dtype=torch.int32, device=dev)
-        for d in (bfs_d[0], sssp_d[0]):
-            cgp.run_batch(graph, [d], opts, out=o1)
+        o1b = opts if args.no_autotune else cgp.autotune(graph, bfs_d[:1], opts, reps=2)
+        o1s = opts if args.no_autotune else cgp.autotune(graph, sssp_d[:1], opts, reps=2)
+        for d, oo in ((bfs_d[0], o1b), (sssp_d[0], o1s)):
+            cgp.run_batch(graph, [d], oo, out=o1)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for d in bfs_d[:nb1]:
-            cgp.run_batch(graph, [d], opts, out=o1)
+            cgp.run_batch(graph, [d], o1b, out=o1)
         e1.record(stream)
         torch.cuda.synchronize()
         tb1 = e0.elapsed_time(e1) / nb1
         e0.record(stream)
         for d in sssp_d[:ns1]:
-            cgp.run_batch(graph, [d], opts, out=o1)
+            cgp.run_batch(graph, [d], o1s, out=o1)
         e1.record(stream)
         torch.cuda.synchronize()
         ts1 = e0.elapsed_time(e1) / ns1
@@ -467,12 +490,13 @@ def main():
     if args.e2e_steps > 0:
         hb = torch.empty((V, len(bfs_d)), dtype=torch.int32, pin_memory=True)
         hs = torch.empty((V, len(sssp_d)), dtype=torch.int32, pin_memory=True)
-        eopts = cgp.RunOptions(**tuning)
+        eopts_b = dataclasses.replace(opts_b, stream=0)
+        eopts_s = dataclasses.replace(opts_s, stream=0)
         def e2e_step():
             if bfs_d:
-                cgp.run_batch(graph, bfs_d, eopts, out=hb)
+                cgp.run_batch(graph, bfs_d, eopts_b, out=hb)
             if sssp_d:
-                cgp.run_batch(graph, sssp_d, eopts, out=hs)
+                cgp.run_batch(graph, sssp_d, eopts_s, out=hs)
         e2e_step()
         barrier()
         t0 = time.perf_counter()
@@ -530,8 +554,12 @@ def main():
                        "V": V, "E": g.num_edges, "weights": "u32 uniform [1,64]",
                        "queries_per_gpu": {"bfs": len(bfs_d), "sssp": len(sssp_d)},
                        "mask_words": W, "largest_component_vertices": comp_v,
-                       "traversal_mode": args.mode, "pull_edge_ratio": args.pull_edge_ratio,
-                       "pull_frontier_ratio": args.pull_frontier_ratio,
+                       "traversal_mode": args.mode,
+                       "tuned": None if args.no_autotune else {
+                           "bfs": {"mask_words": opts_b.mask_words, "heavy_degree": opts_b.heavy_degree,
+                                   "pull_edge_ratio": opts_b.pull_edge_ratio},
+                           "sssp": {"mask_words": opts_s.mask_words, "heavy_degree": opts_s.heavy_degree},
+                           "tuning_s": tune_s},
                        "l2": f"inputs larger than L2: CSR {4 * (V + 1 + 2 * g.num_edges) / 2**20:.0f} MiB "
                              f"+ outputs {8 * V * (len(bfs_d) + len(sssp_d)) / 2**30:.1f} GiB "
                              f"per step, re-initialised every step (no flush)",

@@ -83,7 +83,8 @@ class CgpRequestInfo(Structure):
 class CgpServerStats(Structure):
     _fields_ = [("slots", c_int32), ("active_slots", c_int32), ("queued", c_int64),
                 ("completed", c_int64), ("levels", c_int64), ("busy_ms", c_double),
-                ("state_bytes", c_int64)]
+                ("state_bytes", c_int64), ("admit_ms", c_double), ("retire_ms", c_double),
+                ("retire_passes", c_int64)]
 
 
 # name -> (restype, argtypes)
@@ -102,6 +103,7 @@ SIGNATURES = {
     "cgp_batch_run": (c_int32, [c_void_p, POINTER(CgpQuery), c_int32, POINTER(CgpOptions),
                                 c_void_p, c_int32, c_int32, POINTER(CgpStats)]),
     "cgp_last_profiles": (c_int32, [POINTER(CgpLevelProfile), c_int32, POINTER(c_int32)]),
+    "cgp_autotune": (c_int32, [c_void_p, POINTER(CgpQuery), c_int32, POINTER(CgpOptions), c_int32]),
     "cgp_enactor_create": (c_int32, [c_void_p, POINTER(CgpQuery), c_int32, POINTER(CgpOptions),
                                      POINTER(c_void_p)]),
     "cgp_enactor_destroy": (c_int32, [c_void_p]),

@@ -421,6 +421,20 @@ def run_batch(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpt
                      kernel_profile=kprof, iteration_profiles=profiles, options=options)
 
 
+def autotune(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOptions | None = None,
+             reps: int = 3) -> RunOptions:
+    """Times short runs of `descs` and returns options with the fastest mask
+    width, heavy-vertex threshold and pull threshold (cached per graph and
+    query mix)."""
+    options = options or RunOptions()
+    o = options.to_c()
+    q = _queries_c(list(descs))
+    N.check(N.lib().cgp_autotune(graph.handle, q, len(descs), ctypes.byref(o), reps), "cgp_autotune")
+    return dataclasses.replace(options, mask_words=o.mask_words, heavy_degree=o.heavy_degree,
+                               pull_edge_ratio=o.pull_edge_ratio,
+                               pull_frontier_ratio=o.pull_frontier_ratio)
+
+
 def run(policy: str, graph: CsrGraph, queries, context=None, options: RunOptions | None = None,
         **kw) -> RunResult:
     """puercgp::run<Policy> (run.hxx:11-23): one policy over a batch of sources.

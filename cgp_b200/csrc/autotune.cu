@@ -1,0 +1,132 @@
+// Autotuner: picks the bitmask width (queries per traversal group), the
+// heavy-vertex threshold (degree above which an adjacency list is split into
+// CTA work items) and the push->pull switch threshold for one graph and one
+// query mix, by timing short runs of a representative batch.
+//
+// The reference fixes these: 64-bit masks (puercgp/include/puercgp/core/types.hxx:24),
+// degree buckets at 8/512 (frontier_engine.hxx:945-946) and pull ratios
+// 0.15/0.20 (types.hxx:30-31).  Here they are searched by coordinate descent
+// (pull threshold, then heavy threshold, then mask width), each candidate
+// timed with CUDA events as the median of `reps` runs, and the winner is
+// cached on the graph per (batch size, BFS / SSSP / k-hop counts).
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "engine.h"
+
+namespace cgp {
+namespace {
+
+using TuneKey = std::tuple<const GraphImpl*, int, int, int, int, int>;
+std::mutex g_tune_mu;
+std::map<TuneKey, cgp_options> g_tuned;
+
+float time_run(cgp_graph* g, const cgp_query* q, int n, const cgp_options& o, void* out, int reps,
+               cgp_status* st) {
+  std::vector<float> t;
+  for (int r = 0; r < reps; ++r) {
+    cgp_stats s;
+    *st = cgp_batch_run(g, q, n, &o, out, CGP_LAYOUT_VERTEX_MAJOR, 1, &s);
+    if (*st != CGP_OK) return 1e30f;
+    t.push_back(s.gpu_time_ms);
+  }
+  std::sort(t.begin(), t.end());
+  return t[t.size() / 2];
+}
+
+}  // namespace
+}  // namespace cgp
+
+using namespace cgp;
+
+extern "C" cgp_status cgp_autotune(cgp_graph* graph, const cgp_query* sample, int32_t n,
+                                   cgp_options* opts, int32_t reps) {
+  clear_error();
+  if (graph == nullptr || sample == nullptr || n <= 0 || opts == nullptr)
+    return set_error(CGP_ERR_INVALID_ARG, "NULL argument or empty sample");
+  GraphImpl* g = &graph->impl;
+  int nb = 0, ns = 0, nk = 0;
+  for (int i = 0; i < n; ++i) {
+    nb += sample[i].kind == CGP_KIND_BFS;
+    ns += sample[i].kind == CGP_KIND_SSSP;
+    nk += sample[i].kind == CGP_KIND_KHOP;
+  }
+  const TuneKey key{g, opts->traversal_mode, n, nb, ns, nk};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      void* stream = opts->stream;
+      *opts = it->second;
+      opts->stream = stream;
+      return CGP_OK;
+    }
+  }
+  if (reps <= 0) reps = 3;
+  void* out = nullptr;
+  try {
+    ck(cudaSetDevice(g->device), "cudaSetDevice");
+    ck(cudaMalloc(&out, static_cast<size_t>(g->V) * n * 4), "autotune output");
+  } catch (...) {
+    return translate_exception();
+  }
+  cgp_options best = *opts;
+  best.profile_iterations = 0;
+  best.profile_kernels = 0;
+  cgp_status st = CGP_OK;
+  float best_t = time_run(graph, sample, n, best, out, 1, &st);  // warm-up and capture
+  best_t = time_run(graph, sample, n, best, out, reps, &st);
+  if (st == CGP_OK && nb + nk > 0 && best.traversal_mode == CGP_MODE_HYBRID) {
+    for (double r : {0.005, 0.02, 0.05, 0.1, 0.3}) {
+      cgp_options c = best;
+      c.pull_edge_ratio = r;
+      float t = time_run(graph, sample, n, c, out, reps, &st);
+      if (st != CGP_OK) break;
+      if (t < best_t) {
+        best_t = t;
+        best = c;
+      }
+    }
+  }
+  if (st == CGP_OK) {
+    for (int h : {512, 1024, 4096, 16384}) {
+      cgp_options c = best;
+      c.heavy_degree = h;
+      time_run(graph, sample, n, c, out, 1, &st);  // builds the heavy table once
+      float t = time_run(graph, sample, n, c, out, reps, &st);
+      if (st != CGP_OK) break;
+      if (t < best_t) {
+        best_t = t;
+        best = c;
+      }
+    }
+  }
+  if (st == CGP_OK) {
+    const int wmax = choose_words(nb + ns + nk, 0);
+    for (int w = 1; w < wmax && st == CGP_OK; w <<= 1) {
+      cgp_options c = best;
+      c.mask_words = w;
+      time_run(graph, sample, n, c, out, 1, &st);
+      float t = time_run(graph, sample, n, c, out, reps, &st);
+      if (st != CGP_OK) break;
+      if (t < best_t) {
+        best_t = t;
+        best = c;
+      }
+    }
+  }
+  cudaFree(out);
+  if (st != CGP_OK) return st;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = best;
+  }
+  void* stream = opts->stream;
+  *opts = best;
+  opts->stream = stream;
+  return CGP_OK;
+}

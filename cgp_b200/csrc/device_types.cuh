@@ -75,6 +75,7 @@ struct LevelCtl {
   int32_t profile_cap;
   unsigned long long pull_vertex_threshold;
   unsigned long long pull_edge_threshold;
+  unsigned long long dense_count;  // SSSP vertices queued for the dense kernel this level
   LevelCounters lc;                // counters of the current level
   LevelCounters total;             // sums over all levels
 };
@@ -116,6 +117,7 @@ struct GroupDev {
   uint64_t* planes;    // [K][V*W] depth bit planes
   uint32_t* values;    // [V*Qg] vertex-major values (SSSP, direct depths)
   uint64_t* hacc;      // [n_pheavy*W] pull accumulators of heavy vertices
+  int32_t* dense_list; // [V] SSSP frontier vertices with many active bits
   LevelCtl* ctl;
   LevelProfile* prof;
   const SlotDev* slots;
@@ -129,6 +131,7 @@ struct OutMap {
   int64_t sv;
   int64_t sq;
   const int32_t* qmap;
+  int32_t qmap_contiguous;  // qmap[q] == qmap[0] + q for every q
 };
 
 template <typename OT>

@@ -232,6 +232,7 @@ cgp_status cgp_enactor_read_values(cgp_enactor* e, void* out, int32_t out_layout
     om.sv = qmajor ? 1 : nq;
     om.sq = qmajor ? V : 1;
     om.qmap = e->ws->qmap.as<int32_t>();
+    om.qmap_contiguous = 1;
     group_write_output(e->g, e->ws.get(), e->spec, om, qmajor, e->stream);
     if (!e->wcc_slots.empty()) {
       e->ws->wcc.ensure(static_cast<size_t>(V) * 4);

@@ -169,6 +169,7 @@ void GraphImpl::ensure_heavy(int64_t h, cudaStream_t) {
   build_heavy(hc.row, V, h, heavy);
   build_heavy(symmetric ? hc.row : hc.trow, V, h, pheavy);
   heavy_degree = h;
+  ++heavy_generation;
 }
 
 std::unique_ptr<Workspace> GraphImpl::acquire() {
@@ -252,6 +253,7 @@ struct Grids {
   int tile;   // tile kernels (grid-stride)
   int heavy;
   int clear;
+  int dense;
 };
 
 struct LevelLaunch {
@@ -305,7 +307,8 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
   if (L.has_sssp) {
     if (kt) kt->mark(kClassSsspPush, s);
     k_sssp_push<W, OT, WK><<<t, kBlock, 0, s>>>(L.g, L.G);
-    ++n;
+    k_sssp_dense<W, OT, WK><<<L.gr.dense, kBlock, 0, s>>>(L.g, L.G);
+    n += 2;
     if (L.G.n_heavy) {
       k_sssp_push_heavy<W, OT, WK><<<h, kBlock, 0, s>>>(L.g, L.G);
       ++n;
@@ -320,8 +323,9 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
 
 template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
-  static int tile = 0, heavy = 0;
+  static int tile = 0, heavy = 0, dense = 0;
   if (tile == 0) {
+    dense = occupancy_grid(k_sssp_dense<W, OT, WK>, sms);
     int a = occupancy_grid(k_bfs_push<W, OT, DEPTH>, sms);
     int b = occupancy_grid(k_bfs_pull<W, OT, DEPTH>, sms);
     int c = occupancy_grid(k_sssp_push<W, OT, WK>, sms);
@@ -333,6 +337,7 @@ Grids grids_t(int sms) {
   g.tile = tile;
   g.heavy = heavy;
   g.clear = sms * 4;
+  g.dense = dense;
   return g;
 }
 
@@ -393,6 +398,7 @@ GroupDev group_dev(Workspace* ws, const GroupSpec& spec, bool profiles) {
                  ? nullptr
                  : (spec.external_values ? spec.external_values : ws->values.as<uint32_t>());
   g.hacc = ws->hacc.as<uint64_t>();
+  g.dense_list = ws->dense.as<int32_t>();
   g.ctl = ws->ctl.as<LevelCtl>();
   g.prof = profiles ? ws->prof.as<LevelProfile>() : nullptr;
   g.slots = ws->slots.as<SlotDev>();
@@ -423,6 +429,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   moved |= ws->list1.ensure(static_cast<size_t>(V) * 4);
   moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
   moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, g->pheavy.n)) * W * 8);
+  if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
   if (spec.depth_mode == kDepthPlanes) {
     moved |= ws->planes.ensure(static_cast<size_t>(kInitialPlanes) * mask_bytes);
   } else if (spec.external_values == nullptr) {
@@ -513,7 +520,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
                              (spec.has_bfs ? 1 : 0) | (spec.has_sssp ? 2 : 0) | (L.pull ? 4 : 0) |
                                  (o.profile_iterations ? 8 : 0),
                              levels, spec.Qg, static_cast<int>(g->heavy_degree), ws->generation,
-                             reinterpret_cast<uint64_t>(L.g.values));
+                             reinterpret_cast<uint64_t>(L.g.values), g->heavy_generation);
   auto it = ws->graphs.find(key);
   if (it == ws->graphs.end()) {
     cudaGraph_t graph = nullptr;
@@ -861,6 +868,7 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
     om.sv = qmajor ? 1 : nq;
     om.sq = qmajor ? V : 1;
     om.qmap = nullptr;
+    om.qmap_contiguous = 0;
     // WCC queries: one union-find pass, labels broadcast to every WCC column
     std::vector<int> wcc_idx, trav_idx;
     for (int i = 0; i < nq; ++i) (queries[i].kind == CGP_KIND_WCC ? wcc_idx : trav_idx).push_back(i);
@@ -905,6 +913,8 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
                            cudaMemcpyHostToDevice, s), "upload query map");
         OutMap m = om;
         m.qmap = ws->qmap.as<int32_t>();
+        m.qmap_contiguous = 1;
+        for (int i = 1; i < n; ++i) m.qmap_contiguous &= qmap[i] == qmap[0] + i ? 1 : 0;
         group_write_output(g, ws.get(), spec, m, qmajor, s);
         if (kt) kt->mark(-1, s);
       }

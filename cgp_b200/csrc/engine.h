@@ -89,7 +89,7 @@ struct KernelTimer {
 // invalidates captured CUDA graphs.
 struct Workspace {
   int device = 0;
-  DevBuf visited, fbuf0, fbuf1, list0, list1, stamp, planes, values, hacc;
+  DevBuf visited, fbuf0, fbuf1, list0, list1, stamp, planes, values, hacc, dense;
   DevBuf ctl, prof, slots, stage, wcc, qmap;
   LevelCtl* hctl = nullptr;  // pinned, 2 snapshots
   dev::SlotDev* hslots = nullptr;  // pinned, kMaxWords*64 entries
@@ -97,7 +97,8 @@ struct Workspace {
   cudaStream_t capture = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   uint64_t generation = 1;
-  std::map<std::tuple<int, int, int, int, int, int, int, int, uint64_t, uint64_t>, CachedGraph> graphs;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, uint64_t, uint64_t, uint64_t>,
+           CachedGraph> graphs;
   Workspace(int dev);
   ~Workspace();
   void clear_graphs();
@@ -113,6 +114,7 @@ struct GraphImpl {
   DevBuf row, col, w;      // traversal CSR
   DevBuf trow, tcol;       // transpose (in-edges) for pull on directed graphs
   int64_t heavy_degree = 0;
+  uint64_t heavy_generation = 0;  // bumped on every heavy-table rebuild (captured graphs)
   HeavyTable heavy, pheavy;
   std::mutex mu;
   std::vector<std::unique_ptr<Workspace>> pool;  // idle workspaces

@@ -469,7 +469,7 @@ __device__ __forceinline__ void pull_commit(const GroupDev& g, int64_t V,
 // is found (early exit).  Reads only the current frontier, so depths are
 // exactly level-synchronous.
 template <int W, typename OT, int DEPTH>
-__global__ void __launch_bounds__(kBlock) k_bfs_pull(GroupDev g, DevGraph G) {
+__global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->dir != kDirPull) return;
   const LevelView lv = level_view(g);
@@ -778,18 +778,27 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
     for (int i = 0; i < cnt; ++i) {
       const int32_t nb = __shfl_sync(kFull, nl, i);
       const uint32_t wt = __shfl_sync(kFull, wl, i);
-      uint32_t* row = g.values + static_cast<size_t>(nb) * Qg;
+      uint32_t* row = g.values + static_cast<size_t>(nb) * Qg + lane;
+      // all loads of the active chunks first (independent, in flight together),
+      // then the atomics where a candidate improves, then the ballots
+      uint32_t cur[2 * W];
+#pragma unroll
+      for (int c = 0; c < 2 * W; ++c)
+        cur[c] = (half[c] != 0 && ((half[c] >> lane) & 1u)) ? row[32 * c] : 0u;
+      bool imp[2 * W];
+#pragma unroll
+      for (int c = 0; c < 2 * W; ++c) {
+        imp[c] = false;
+        if (half[c] != 0 && ((half[c] >> lane) & 1u)) {
+          const uint32_t cand = relax_w<WK>(du[c], wt);
+          if (cand < cur[c]) imp[c] = cand < atomicMin(row + 32 * c, cand);
+        }
+      }
       bool any = false;
 #pragma unroll
       for (int c = 0; c < 2 * W; ++c) {
         if (half[c] == 0) continue;
-        bool imp = false;
-        if ((half[c] >> lane) & 1u) {
-          const uint32_t cand = relax_w<WK>(du[c], wt);
-          uint32_t* dst = row + 32 * c + lane;
-          if (cand < *dst) imp = cand < atomicMin(dst, cand);
-        }
-        const unsigned m = __ballot_sync(kFull, imp);
+        const unsigned m = __ballot_sync(kFull, imp[c]);
         if (m) {
           any = true;
           if (lane == 0) {
@@ -806,6 +815,35 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
                   lane);
     }
   }
+}
+
+// Dense SSSP vertices of a level, one warp per vertex (the tile kernel
+// queued them), so that this loop gets a register budget of its own.
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock, 4) k_sssp_dense(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done) return;
+  const LevelView lv = level_view(g);
+  const unsigned long long n = ctl->dense_count;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long improved = 0;
+  for (unsigned long long i = gw; i < n; i += nwarps) {
+    const int32_t u = g.dense_list[i];
+    const int64_t beg = row_at<OT>(G.row, u);
+    const int64_t end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
+    uint64_t b[W];
+    load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
+#pragma unroll
+    for (int k = 0; k < W; ++k) b[k] &= ctl->sssp_bits[k];
+    sssp_dense_edges<W, OT, WK>(g, G, lv, u, b, beg, end, lane, uni, improved);
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(improved, &g.ctl->lc.improved, lane);
 }
 
 // SSSP push over the frontier list: the (edge, active query) pairs of a tile
@@ -857,18 +895,17 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
     const bool work = valid && k > 0 && deg > 0 && deg <= G.heavy_degree;
     spairs += work ? static_cast<unsigned long long>(k) * static_cast<unsigned long long>(deg) : 0ULL;
     sactive += static_cast<unsigned long long>(k);
-    // vertices with many active queries: the whole warp, one at a time
-    unsigned dense = __ballot_sync(kFull, work && k > kDenseBits);
-    while (dense) {
-      const int src = __ffs(dense) - 1;
-      dense &= dense - 1;
-      const int32_t bu = __shfl_sync(kFull, u, src);
-      const int64_t bb = __shfl_sync(kFull, beg, src);
-      const int64_t be = __shfl_sync(kFull, end, src);
-      uint64_t bbits[W];
-#pragma unroll
-      for (int i = 0; i < W; ++i) bbits[i] = __shfl_sync(kFull, b[i], src);
-      sssp_dense_edges<W, OT, WK>(g, G, lv, bu, bbits, bb, be, lane, uni, improved);
+    // vertices with many active queries go to the dense kernel
+    {
+      const bool dq = work && k > kDenseBits;
+      const unsigned m = __ballot_sync(kFull, dq);
+      if (m) {
+        unsigned long long base = 0;
+        if (lane == __ffs(m) - 1)
+          base = atomicAdd(&g.ctl->dense_count, static_cast<unsigned long long>(__popc(m)));
+        base = __shfl_sync(kFull, base, __ffs(m) - 1);
+        if (dq) g.dense_list[base + __popc(m & ((1u << lane) - 1u))] = u;
+      }
     }
     // the rest: (edge, query) pairs flattened over the lanes
     long long wk = (work && k <= kDenseBits) ? static_cast<long long>(k) * deg : 0;
@@ -1080,6 +1117,7 @@ __global__ void k_level_end(GroupDev g) {
   ctl->total.sssp_active += ctl->lc.sssp_active;
   ctl->total.improved += ctl->lc.improved;
   ctl->lc = LevelCounters{0, 0, 0, 0, 0, 0};
+  ctl->dense_count = 0;
   ctl->total_frontier += ctl->count[par];
   ctl->total_edges += ctl->edges[par];
   if (ctl->dir == kDirPush) ctl->push_levels++;
@@ -1196,13 +1234,40 @@ __global__ void k_materialize_planes(const uint64_t* visited, const uint64_t* pl
     return;
   }
   if (blockIdx.y != 0) return;
+  // vertex-major: each lane owns 8 consecutive queries of a 256-query block,
+  // loads their visited word and the K plane words once, and writes the 8
+  // depths (two 16-byte stores when the columns are contiguous and aligned).
   const int lane = threadIdx.x & 31;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  const bool vec = om.qmap_contiguous && (om.sv % 4 == 0) && om.sq == 1 && (om.qmap[0] % 4 == 0);
   for (int64_t v = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; v < V;
        v += warps) {
     uint32_t* row = om.out + v * om.sv;
-    for (int q = lane; q < Qg; q += 32)
-      row[static_cast<int64_t>(om.qmap[q]) * om.sq] = plane_depth<W>(visited, planes, K, V, v, q);
+    for (int q0 = 8 * lane; q0 < Qg; q0 += 256) {
+      const size_t word = static_cast<size_t>(v) * W + (q0 >> 6);
+      const int sh = q0 & 63;
+      const uint32_t vis = static_cast<uint32_t>(visited[word] >> sh) & 0xffu;
+      uint32_t d[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) d[j] = 0;
+      for (int b = 0; b < K; ++b) {
+        const uint32_t pl =
+            static_cast<uint32_t>(planes[static_cast<size_t>(b) * V * W + word] >> sh) & 0xffu;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) d[j] |= ((pl >> j) & 1u) << b;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (!((vis >> j) & 1u)) d[j] = 0x7fffffffu;
+      if (vec && q0 + 8 <= Qg) {
+        uint4* dst = reinterpret_cast<uint4*>(row + om.qmap[q0]);
+        dst[0] = make_uint4(d[0], d[1], d[2], d[3]);
+        dst[1] = make_uint4(d[4], d[5], d[6], d[7]);
+      } else {
+        for (int j = 0; j < 8 && q0 + j < Qg; ++j)
+          row[static_cast<int64_t>(om.qmap[q0 + j]) * om.sq] = d[j];
+      }
+    }
   }
 }
 

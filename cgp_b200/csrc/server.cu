@@ -188,6 +188,9 @@ struct cgp_server {
   int64_t completed = 0;
   int64_t levels = 0;
   double busy_ms = 0;
+  double admit_ms = 0;
+  double retire_ms = 0;
+  int64_t retire_passes = 0;
   int64_t state_bytes = 0;
   bool wcc_ready = false;
   std::string fatal;
@@ -248,6 +251,7 @@ GroupDev server_dev(cgp_server* sv) {
   g.planes = nullptr;
   g.values = ws->values.as<uint32_t>();
   g.hacc = ws->hacc.as<uint64_t>();
+  g.dense_list = ws->dense.as<int32_t>();
   g.ctl = ws->ctl.as<LevelCtl>();
   g.prof = nullptr;
   g.slots = ws->slots.as<SlotDev>();
@@ -289,6 +293,7 @@ void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
 }
 
 void cgp_server::retire(std::vector<int>& to_retire, bool forced) {
+  const double t_start = now_ms();
   const int64_t V = g->V;
   const uint32_t f32 = g->weight_kind == CGP_WEIGHT_F32 ? 1u : 0u;
   RetireFn rf = pick_retire(W);
@@ -339,8 +344,10 @@ void cgp_server::retire(std::vector<int>& to_retire, bool forced) {
       --active;
       ++completed;
     }
+    ++retire_passes;
     done_cv.notify_all();
   }
+  retire_ms += now_ms() - t_start;
 }
 
 void cgp_server::loop() {
@@ -396,6 +403,7 @@ void cgp_server::loop() {
       }
       finish_wcc(wcc_tickets);
       if (nadmit > 0) {
+        const double ta = now_ms();
         LevelCtl c;
         ck(cudaMemcpyAsync(&c.level, reinterpret_cast<char*>(ws->ctl.p) + offsetof(LevelCtl, level),
                            sizeof(int32_t), cudaMemcpyDeviceToHost, stream), "read level");
@@ -406,6 +414,7 @@ void cgp_server::loop() {
         ck(cudaStreamSynchronize(stream), "admit");
         std::lock_guard<std::mutex> lk(mu);
         for (int i = 0; i < nadmit; ++i) reqs[slot_ticket[h_admit[i].slot]].admit_level = c.level;
+        admit_ms += now_ms() - ta;
       }
       int act;
       {
@@ -640,6 +649,9 @@ cgp_status cgp_server_get_stats(cgp_server* sv, cgp_server_stats* st) {
   st->levels = sv->levels;
   st->busy_ms = sv->busy_ms;
   st->state_bytes = sv->state_bytes;
+  st->admit_ms = sv->admit_ms;
+  st->retire_ms = sv->retire_ms;
+  st->retire_passes = sv->retire_passes;
   return CGP_OK;
 }
 

@@ -213,6 +213,17 @@ cgp_status cgp_batch_run(cgp_graph* g, const cgp_query* queries, int32_t nq,
                          const cgp_options* opts, void* out, int32_t out_layout,
                          int32_t out_on_device, cgp_stats* stats);
 
+/* Autotuner: times short runs of `sample` (a representative batch) and
+ * writes the fastest mask width (mask_words: queries per traversal group),
+ * heavy_degree and pull_edge_ratio into *opts, starting from *opts.  The
+ * choice is cached on the graph per (traversal mode, batch size, BFS / SSSP
+ * / k-hop counts); `reps` runs per candidate (0 = 3).  Replaces the
+ * reference's fixed 64-bit masks, degree buckets and pull ratios
+ * (puercgp/include/puercgp/core/types.hxx:24,30-31,
+ * puercgp/include/puercgp/engine/frontier_engine.hxx:945-946). */
+cgp_status cgp_autotune(cgp_graph* g, const cgp_query* sample, int32_t n,
+                        cgp_options* opts, int32_t reps);
+
 /* Per-level profiles of the last cgp_batch_run on this thread (group 0). */
 cgp_status cgp_last_profiles(cgp_level_profile* out, int32_t cap, int32_t* count);
 cgp_status cgp_last_kernel_profile(cgp_kernel_profile* out);
@@ -319,9 +330,12 @@ typedef struct {
   int32_t active_slots;
   int64_t queued;
   int64_t completed;
-  int64_t levels;
-  double busy_ms;
+  int64_t levels;            /* levels run since creation                           */
+  double busy_ms;            /* host time spent running levels                       */
   int64_t state_bytes;
+  double admit_ms;           /* host time spent admitting requests                   */
+  double retire_ms;          /* host time spent retiring slots and copying results   */
+  int64_t retire_passes;     /* snapshot-and-reset passes over the vertices          */
 } cgp_server_stats;
 cgp_status cgp_server_get_stats(cgp_server* s, cgp_server_stats* st);
 

@@ -336,3 +336,21 @@ def test_invalid_batches_raise(rmat_u32):
         cgp.run("bfs", graph, [g.num_vertices])
     with pytest.raises(ValueError):
         cgp.run("bfs", graph, [1, 2, 3], options=cgp.RunOptions(max_queries=2))
+
+
+def test_autotune_keeps_results_and_caches(rmat_u32):
+    import time
+    g, graph = rmat_u32
+    src = g.pick_sources(160, seed=21)
+    descs = [cgp.QueryDescriptor(int(s), "bfs" if i % 2 else "sssp") for i, s in enumerate(src)]
+    t0 = time.perf_counter()
+    opts = cgp.autotune(graph, descs, reps=1)
+    t1 = time.perf_counter()
+    again = cgp.autotune(graph, descs, reps=1)
+    t2 = time.perf_counter()
+    assert again == opts and (t2 - t1) < (t1 - t0)
+    assert opts.mask_words in (0, 1, 2, 4) and opts.heavy_degree >= 0
+    r = cgp.run_batch(graph, descs, opts, layout="query")
+    for i, d in enumerate(descs):
+        exp = oracle.bfs(g, d.source).view(np.uint32) if d.kind == "bfs" else oracle.sssp(g, d.source)
+        np.testing.assert_array_equal(r.values[i], exp)
