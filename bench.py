@@ -64,6 +64,8 @@ def parse_args():
     p.add_argument("--serve-rates", default="500,2000,8000")
     p.add_argument("--serve-seconds", type=float, default=3.0)
     p.add_argument("--serve-slots", type=int, default=256)
+    p.add_argument("--serve-profile", action="store_true",
+                   help="time the serving loop's kernel classes (slower: no CUDA graphs)")
     return p.parse_args()
 
 
@@ -302,7 +304,10 @@ def run_serve(args):
     descs = serve_mix(g, 4096, seed=42)
     rows = []
     with cgp.Server(graph, slots=args.serve_slots,
-                    options=cgp.RunOptions(traversal_mode=args.mode)) as srv:
+                    options=cgp.RunOptions(traversal_mode=args.mode,
+                                           pull_edge_ratio=args.pull_edge_ratio,
+                                           heavy_degree=args.heavy_degree,
+                                           profile_kernels=args.serve_profile)) as srv:
         poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
             s0 = srv.stats()
@@ -313,6 +318,9 @@ def run_serve(args):
             row["retire_ms"] = s1["retire_ms"] - s0["retire_ms"]
             row["retire_passes"] = s1["retire_passes"] - s0["retire_passes"]
             row["admit_ms"] = s1["admit_ms"] - s0["admit_ms"]
+            if args.serve_profile:
+                row["kernel_ms"] = {k: s1["kernel_ms"].get(k, 0) - s0["kernel_ms"].get(k, 0)
+                                    for k in s1["kernel_ms"]}
             rows.append(row)
         st = srv.stats()
     line = {"metric": "serve p50/p99 latency", "unit": "ms", "workload":

@@ -84,7 +84,7 @@ class CgpServerStats(Structure):
     _fields_ = [("slots", c_int32), ("active_slots", c_int32), ("queued", c_int64),
                 ("completed", c_int64), ("levels", c_int64), ("busy_ms", c_double),
                 ("state_bytes", c_int64), ("admit_ms", c_double), ("retire_ms", c_double),
-                ("retire_passes", c_int64)]
+                ("retire_passes", c_int64), ("kernel_ms", c_double * 8)]
 
 
 # name -> (restype, argtypes)

@@ -612,7 +612,10 @@ class Server:
     def stats(self) -> dict:
         s = N.CgpServerStats()
         N.check(N.lib().cgp_server_get_stats(self._h, ctypes.byref(s)), "stats")
-        return {k: getattr(s, k) for k, _ in N.CgpServerStats._fields_}
+        d = {k: getattr(s, k) for k, _ in N.CgpServerStats._fields_ if k != "kernel_ms"}
+        d["kernel_ms"] = {name: s.kernel_ms[i] for i, name in enumerate(N.KERNEL_CLASSES)
+                          if s.kernel_ms[i] > 0}
+        return d
 
     def close(self):
         if getattr(self, "_h", None):

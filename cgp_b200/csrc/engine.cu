@@ -109,7 +109,8 @@ void KernelTimer::flush() {
 }
 
 // --------------------------------------------------------------- graph
-DevGraph GraphImpl::dev_graph() const {
+DevGraph GraphImpl::dev_graph(int64_t h) {
+  const HeavyPair& hp = heavy_for(h);
   DevGraph d;
   d.row = row.p;
   d.col = col.as<int32_t>();
@@ -118,15 +119,15 @@ DevGraph GraphImpl::dev_graph() const {
   d.pcol = pull_col();
   d.V = V;
   d.E = E;
-  d.heavy = heavy.vertices.as<int32_t>();
-  d.heavy_chunk_start = heavy.chunk_start.as<int64_t>();
-  d.n_heavy = heavy.n;
-  d.heavy_chunks = heavy.chunks;
-  d.pheavy = pheavy.vertices.as<int32_t>();
-  d.pheavy_chunk_start = pheavy.chunk_start.as<int64_t>();
-  d.n_pheavy = pheavy.n;
-  d.pheavy_chunks = pheavy.chunks;
-  d.heavy_degree = heavy_degree;
+  d.heavy = hp.heavy.vertices.as<int32_t>();
+  d.heavy_chunk_start = hp.heavy.chunk_start.as<int64_t>();
+  d.n_heavy = hp.heavy.n;
+  d.heavy_chunks = hp.heavy.chunks;
+  d.pheavy = hp.pheavy.vertices.as<int32_t>();
+  d.pheavy_chunk_start = hp.pheavy.chunk_start.as<int64_t>();
+  d.n_pheavy = hp.pheavy.n;
+  d.pheavy_chunks = hp.pheavy.chunks;
+  d.heavy_degree = h;
   return d;
 }
 
@@ -162,14 +163,18 @@ void build_heavy(const std::vector<int64_t>& row, int64_t V, int64_t h, HeavyTab
 
 }  // namespace
 
-void GraphImpl::ensure_heavy(int64_t h, cudaStream_t) {
-  if (h == heavy_degree && heavy.chunk_start.p) return;
-  std::lock_guard<std::mutex> lk(g_host_mu);
-  HostCsr& hc = g_host[this];
-  build_heavy(hc.row, V, h, heavy);
-  build_heavy(symmetric ? hc.row : hc.trow, V, h, pheavy);
-  heavy_degree = h;
-  ++heavy_generation;
+const HeavyPair& GraphImpl::heavy_for(int64_t h) {
+  std::lock_guard<std::mutex> lk(heavy_mu);
+  auto it = heavy_cache.find(h);
+  if (it != heavy_cache.end()) return *it->second;
+  auto hp = std::make_unique<HeavyPair>();
+  {
+    std::lock_guard<std::mutex> hl(g_host_mu);
+    HostCsr& hc = g_host[this];
+    build_heavy(hc.row, V, h, hp->heavy);
+    build_heavy(symmetric ? hc.row : hc.trow, V, h, hp->pheavy);
+  }
+  return *heavy_cache.emplace(h, std::move(hp)).first->second;
 }
 
 std::unique_ptr<Workspace> GraphImpl::acquire() {
@@ -408,18 +413,14 @@ GroupDev group_dev(Workspace* ws, const GroupSpec& spec, bool profiles) {
 
 constexpr int kProfileCap = 1 << 16;
 
-int64_t auto_heavy_degree(const cgp_options& o) {
-  if (o.heavy_degree > 0) return std::min<int64_t>(o.heavy_degree, 1 << 20);
-  return 2048;
-}
-
 }  // namespace
 
 void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
                    cudaStream_t s) {
   const int64_t V = g->V;
   const int W = spec.W;
-  g->ensure_heavy(auto_heavy_degree(o), s);
+  const int64_t hth = heavy_threshold(o);
+  const HeavyPair& hp = g->heavy_for(hth);
   bool moved = false;
   const size_t mask_bytes = static_cast<size_t>(V) * W * 8;
   moved |= ws->visited.ensure(mask_bytes);
@@ -428,7 +429,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   moved |= ws->list0.ensure(static_cast<size_t>(V) * 4);
   moved |= ws->list1.ensure(static_cast<size_t>(V) * 4);
   moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
-  moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, g->pheavy.n)) * W * 8);
+  moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8);
   if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
   if (spec.depth_mode == kDepthPlanes) {
     moved |= ws->planes.ensure(static_cast<size_t>(kInitialPlanes) * mask_bytes);
@@ -444,7 +445,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   ck(cudaMemsetAsync(ws->fbuf0.p, 0, mask_bytes, s), "memset frontier");
   ck(cudaMemsetAsync(ws->fbuf1.p, 0, mask_bytes, s), "memset next frontier");
   ck(cudaMemsetAsync(ws->stamp.p, 0xff, static_cast<size_t>(V) * 4, s), "memset stamp");
-  ck(cudaMemsetAsync(ws->hacc.p, 0, static_cast<size_t>(std::max(1, g->pheavy.n)) * W * 8, s),
+  ck(cudaMemsetAsync(ws->hacc.p, 0, static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8, s),
      "memset hacc");
   if (spec.depth_mode == kDepthPlanes)
     ck(cudaMemsetAsync(ws->planes.p, 0, static_cast<size_t>(kInitialPlanes) * mask_bytes, s),
@@ -488,7 +489,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
     spec.launches++;
   }
   Dispatch d = dispatch(W, g->offset_bytes, spec.depth_mode, g->weight_kind);
-  d.seed(group_dev(ws, spec, o.profile_iterations != 0), g->dev_graph(), s);
+  d.seed(group_dev(ws, spec, o.profile_iterations != 0), g->dev_graph(hth), s);
   ck(cudaGetLastError(), "seed");
   spec.launches++;
 }
@@ -501,7 +502,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   Dispatch d = dispatch(spec.W, g->offset_bytes, spec.depth_mode, g->weight_kind);
   LevelLaunch L;
   L.g = group_dev(ws, spec, o.profile_iterations != 0);
-  L.G = g->dev_graph();
+  L.G = g->dev_graph(heavy_threshold(o));
   L.gr = d.grids(g->num_sms);
   L.has_bfs = spec.has_bfs;
   L.has_sssp = spec.has_sssp;
@@ -519,8 +520,8 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   auto key = std::make_tuple(spec.W, g->offset_bytes, spec.depth_mode, g->weight_kind,
                              (spec.has_bfs ? 1 : 0) | (spec.has_sssp ? 2 : 0) | (L.pull ? 4 : 0) |
                                  (o.profile_iterations ? 8 : 0),
-                             levels, spec.Qg, static_cast<int>(g->heavy_degree), ws->generation,
-                             reinterpret_cast<uint64_t>(L.g.values), g->heavy_generation);
+                             levels, spec.Qg, static_cast<int>(L.G.heavy_degree), ws->generation,
+                             reinterpret_cast<uint64_t>(L.g.values));
   auto it = ws->graphs.find(key);
   if (it == ws->graphs.end()) {
     cudaGraph_t graph = nullptr;

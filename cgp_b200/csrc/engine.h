@@ -49,6 +49,17 @@ struct HeavyTable {
   int64_t chunks = 0;
 };
 
+// Heavy tables of the traversal CSR and of the pull CSR for one threshold.
+struct HeavyPair {
+  HeavyTable heavy, pheavy;
+};
+
+// Degree above which adjacency lists are split into CTA work items.
+inline int64_t heavy_threshold(const cgp_options& o) {
+  if (o.heavy_degree > 0) return o.heavy_degree < (1 << 20) ? o.heavy_degree : (1 << 20);
+  return 2048;
+}
+
 using LevelCtl = dev::LevelCtl;
 
 struct CachedGraph {
@@ -97,8 +108,8 @@ struct Workspace {
   cudaStream_t capture = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   uint64_t generation = 1;
-  std::map<std::tuple<int, int, int, int, int, int, int, int, uint64_t, uint64_t, uint64_t>,
-           CachedGraph> graphs;
+  std::map<std::tuple<int, int, int, int, int, int, int, int, uint64_t, uint64_t>, CachedGraph>
+      graphs;
   Workspace(int dev);
   ~Workspace();
   void clear_graphs();
@@ -113,16 +124,16 @@ struct GraphImpl {
   bool symmetric = false;
   DevBuf row, col, w;      // traversal CSR
   DevBuf trow, tcol;       // transpose (in-edges) for pull on directed graphs
-  int64_t heavy_degree = 0;
-  uint64_t heavy_generation = 0;  // bumped on every heavy-table rebuild (captured graphs)
-  HeavyTable heavy, pheavy;
   std::mutex mu;
+  std::mutex heavy_mu;
+  std::map<int64_t, std::unique_ptr<HeavyPair>> heavy_cache;  // built once per threshold
   std::vector<std::unique_ptr<Workspace>> pool;  // idle workspaces
 
   const void* pull_row() const { return symmetric ? row.p : trow.p; }
   const int32_t* pull_col() const { return symmetric ? col.as<int32_t>() : tcol.as<int32_t>(); }
-  dev::DevGraph dev_graph() const;
-  void ensure_heavy(int64_t h, cudaStream_t s);
+  // Heavy tables for threshold h (built on first use, then kept).
+  const HeavyPair& heavy_for(int64_t h);
+  dev::DevGraph dev_graph(int64_t h);
   std::unique_ptr<Workspace> acquire();
   void release(std::unique_ptr<Workspace> ws);
 };

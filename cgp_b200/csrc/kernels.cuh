@@ -510,16 +510,24 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
     const bool work = valid && !heavy && deg > 0 && mask_any<W>(need);
     pverts += work ? 1 : 0;
     if (work && deg <= 32) {
-      for (int64_t e = beg; e < end; ++e) {
-        ++pedges;
-        uint64_t fu[W];
-        load_mask<W>(lv.fcur + static_cast<size_t>(G.pcol[e]) * W, fu);
+      // four in-edges per step: their column and mask loads are independent
+      // and stay in flight together; early exit is checked once per step
+      for (int64_t e = beg; e < end; e += 4) {
+        int32_t us[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) us[j] = (e + j < end) ? G.pcol[e + j] : -1;
+        pedges += static_cast<unsigned long long>(end - e < 4 ? end - e : 4);
         bool full = true;
 #pragma unroll
-        for (int i = 0; i < W; ++i) {
-          acc[i] |= fu[i] & need[i];
-          full &= acc[i] == need[i];
+        for (int j = 0; j < 4; ++j) {
+          if (us[j] < 0) continue;
+          uint64_t fu[W];
+          load_mask<W>(lv.fcur + static_cast<size_t>(us[j]) * W, fu);
+#pragma unroll
+          for (int i = 0; i < W; ++i) acc[i] |= fu[i] & need[i];
         }
+#pragma unroll
+        for (int i = 0; i < W; ++i) full &= acc[i] == need[i];
         if (full) break;
       }
     }
@@ -759,12 +767,12 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
   const size_t Qg = static_cast<size_t>(g.Qg);
   uint32_t half[2 * W];
   uint32_t du[2 * W];
+  bool act[2 * W];
 #pragma unroll
   for (int c = 0; c < 2 * W; ++c) {
     half[c] = static_cast<uint32_t>(bits[c >> 1] >> (32 * (c & 1)));
-    du[c] = ((half[c] >> lane) & 1u)
-                ? g.values[static_cast<size_t>(u) * Qg + 32 * c + lane]
-                : 0xffffffffu;
+    act[c] = (half[c] >> lane) & 1u;
+    du[c] = act[c] ? g.values[static_cast<size_t>(u) * Qg + 32 * c + lane] : 0xffffffffu;
   }
   for (int64_t e0 = eb; e0 < ee; e0 += 32) {
     const int64_t e = e0 + lane;
@@ -779,26 +787,27 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
       const int32_t nb = __shfl_sync(kFull, nl, i);
       const uint32_t wt = __shfl_sync(kFull, wl, i);
       uint32_t* row = g.values + static_cast<size_t>(nb) * Qg + lane;
-      // all loads of the active chunks first (independent, in flight together),
-      // then the atomics where a candidate improves, then the ballots
+      // all loads of the active chunks first (independent, in flight together);
+      // improvements are rare, so the atomics and ballots run only when some
+      // lane of the warp has a better candidate for this edge
       uint32_t cur[2 * W];
 #pragma unroll
-      for (int c = 0; c < 2 * W; ++c)
-        cur[c] = (half[c] != 0 && ((half[c] >> lane) & 1u)) ? row[32 * c] : 0u;
-      bool imp[2 * W];
+      for (int c = 0; c < 2 * W; ++c) cur[c] = act[c] ? row[32 * c] : 0u;
+      uint32_t cand[2 * W];
+      bool better = false;
 #pragma unroll
       for (int c = 0; c < 2 * W; ++c) {
-        imp[c] = false;
-        if (half[c] != 0 && ((half[c] >> lane) & 1u)) {
-          const uint32_t cand = relax_w<WK>(du[c], wt);
-          if (cand < cur[c]) imp[c] = cand < atomicMin(row + 32 * c, cand);
-        }
+        cand[c] = relax_w<WK>(du[c], wt);
+        better |= act[c] && cand[c] < cur[c];
       }
+      if (!__any_sync(kFull, better)) continue;
       bool any = false;
 #pragma unroll
       for (int c = 0; c < 2 * W; ++c) {
         if (half[c] == 0) continue;
-        const unsigned m = __ballot_sync(kFull, imp[c]);
+        bool imp = false;
+        if (act[c] && cand[c] < cur[c]) imp = cand[c] < atomicMin(row + 32 * c, cand[c]);
+        const unsigned m = __ballot_sync(kFull, imp);
         if (m) {
           any = true;
           if (lane == 0) {
@@ -1250,7 +1259,18 @@ __global__ void k_materialize_planes(const uint64_t* visited, const uint64_t* pl
       uint32_t d[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) d[j] = 0;
-      for (int b = 0; b < K; ++b) {
+      // the first 8 planes are loaded together, then folded in
+      uint64_t pw[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        pw[b] = b < K ? planes[static_cast<size_t>(b) * V * W + word] : 0ULL;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const uint32_t pl = static_cast<uint32_t>(pw[b] >> sh) & 0xffu;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) d[j] |= ((pl >> j) & 1u) << b;
+      }
+      for (int b = 8; b < K; ++b) {
         const uint32_t pl =
             static_cast<uint32_t>(planes[static_cast<size_t>(b) * V * W + word] >> sh) & 0xffu;
 #pragma unroll

@@ -106,35 +106,57 @@ __global__ void k_admit(GroupDev g, DevGraph G, const AdmitReq* reqs, int n) {
 
 // Retires slots: snapshot each slot column (mapped to its kind's unreached
 // marker) into staging row i, reset the column, and clear the slots' visited
-// bits (and frontier bits when a running request was cancelled).
+// bits (and frontier bits when a running request was cancelled).  A CTA
+// takes 64 vertices: its warps read the retiring slots of one vertex row
+// together (lane i <-> slot i, all within the row's 1 KB), stage them in
+// shared memory, and then write every slot's staging row contiguously.
+constexpr int kRetireTile = 64;
+
 template <int W>
-__global__ void k_retire(GroupDev g, int64_t V, const RetireReq* reqs, int n,
-                         uint32_t* staging, const uint64_t* clear, int clear_frontier,
-                         uint32_t f32) {
-  for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
-       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    uint32_t* row = g.values + static_cast<size_t>(v) * g.Qg;
-    for (int i = 0; i < n; ++i) {
-      const RetireReq r = reqs[i];
-      uint32_t x = row[r.slot];
-      row[r.slot] = kServeInf;
-      if (r.has_out) {
+__global__ void __launch_bounds__(kBlock) k_retire(GroupDev g, int64_t V, const RetireReq* reqs,
+                                                   int n, uint32_t* staging, const uint64_t* clear,
+                                                   int clear_frontier, uint32_t f32) {
+  __shared__ uint32_t tile[kRetireBatch][kRetireTile + 1];
+  __shared__ RetireReq rq[kRetireBatch];
+  if (threadIdx.x < n) rq[threadIdx.x] = reqs[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  bool any_out = false;
+  for (int i = 0; i < n; ++i) any_out |= rq[i].has_out != 0;
+  for (int64_t v0 = static_cast<int64_t>(blockIdx.x) * kRetireTile; v0 < V;
+       v0 += static_cast<int64_t>(gridDim.x) * kRetireTile) {
+    for (int j = wib; j < kRetireTile; j += kWarpsPerBlock) {
+      const int64_t v = v0 + j;
+      if (v >= V) break;
+      uint32_t* row = g.values + static_cast<size_t>(v) * g.Qg;
+      if (lane < n) {
+        const RetireReq r = rq[lane];
+        uint32_t x = row[r.slot];
+        row[r.slot] = kServeInf;
         if (x == kServeInf) {
           if (r.kind == 0 || r.kind == 3) x = 0x7fffffffu;
           else if (f32) x = 0x7f800000u;
         }
-        staging[static_cast<size_t>(i) * V + v] = x;
+        tile[lane][j] = x;
+      }
+      if (lane < W && clear[lane]) {
+        const size_t wi = static_cast<size_t>(v) * W + lane;
+        g.visited[wi] &= ~clear[lane];
+        if (clear_frontier) {
+          g.fbuf0[wi] &= ~clear[lane];
+          g.fbuf1[wi] &= ~clear[lane];
+        }
       }
     }
-    uint64_t* vis = g.visited + static_cast<size_t>(v) * W;
-    for (int w = 0; w < W; ++w) {
-      if (!clear[w]) continue;
-      vis[w] &= ~clear[w];
-      if (clear_frontier) {
-        g.fbuf0[static_cast<size_t>(v) * W + w] &= ~clear[w];
-        g.fbuf1[static_cast<size_t>(v) * W + w] &= ~clear[w];
+    __syncthreads();
+    if (any_out) {
+      for (int t = threadIdx.x; t < n * kRetireTile; t += blockDim.x) {
+        const int i = t / kRetireTile, j = t % kRetireTile;
+        if (rq[i].has_out && v0 + j < V) staging[static_cast<size_t>(i) * V + v0 + j] = tile[i][j];
       }
     }
+    __syncthreads();
   }
 }
 
@@ -198,6 +220,7 @@ struct cgp_server {
   AdmitReq* h_admit = nullptr;
   RetireReq* h_retire = nullptr;
   uint64_t* h_clear = nullptr;
+  std::unique_ptr<KernelTimer> kt;  // per-class kernel times (profile_kernels)
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
 
   double now_ms() const {
@@ -320,7 +343,7 @@ void cgp_server::retire(std::vector<int>& to_retire, bool forced) {
     ck(cudaMemcpyAsync(clear_dev.p, h_clear, kMaxWords * 8, cudaMemcpyHostToDevice, stream),
        "upload clear");
     rf(server_dev(this), V, retire_dev.as<RetireReq>(), n, staging.as<uint32_t>(),
-       clear_dev.as<uint64_t>(), forced ? 1 : 0, f32, g->num_sms * 8, stream);
+       clear_dev.as<uint64_t>(), forced ? 1 : 0, f32, g->num_sms * 4, stream);
     ck(cudaGetLastError(), "retire");
     for (int i = 0; i < n; ++i) {
       if (h_retire[i].has_out)
@@ -409,7 +432,8 @@ void cgp_server::loop() {
                            sizeof(int32_t), cudaMemcpyDeviceToHost, stream), "read level");
         ck(cudaMemcpyAsync(admit_dev.p, h_admit, nadmit * sizeof(AdmitReq), cudaMemcpyHostToDevice,
                            stream), "upload admits");
-        af(server_dev(this), g->dev_graph(), admit_dev.as<AdmitReq>(), nadmit, stream);
+        af(server_dev(this), g->dev_graph(heavy_threshold(o)), admit_dev.as<AdmitReq>(), nadmit,
+           stream);
         ck(cudaGetLastError(), "admit");
         ck(cudaStreamSynchronize(stream), "admit");
         std::lock_guard<std::mutex> lk(mu);
@@ -424,7 +448,8 @@ void cgp_server::loop() {
       if (act == 0) continue;
       const double tb = now_ms();
       GroupRun r;
-      group_enact(g, ws.get(), spec, o, stream, &r, per);
+      group_enact(g, ws.get(), spec, o, stream, &r, per, kt.get());
+      if (kt) kt->flush();
       LevelCtl c;
       ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
       busy_ms += now_ms() - tb;
@@ -518,6 +543,7 @@ cgp_status cgp_server_create(cgp_graph* graph, int32_t slots, const cgp_options*
     ck(cudaHostAlloc(reinterpret_cast<void**>(&sv->h_clear), kMaxWords * 8, cudaHostAllocDefault),
        "pinned");
     ck(cudaStreamSynchronize(sv->stream), "server init");
+    if (sv->o.profile_kernels) sv->kt = std::make_unique<KernelTimer>();
     sv->th = std::thread([sv] { sv->loop(); });
     *out = sv;
     return CGP_OK;
@@ -652,6 +678,7 @@ cgp_status cgp_server_get_stats(cgp_server* sv, cgp_server_stats* st) {
   st->admit_ms = sv->admit_ms;
   st->retire_ms = sv->retire_ms;
   st->retire_passes = sv->retire_passes;
+  for (int c = 0; c < 8; ++c) st->kernel_ms[c] = sv->kt && c < kNumClasses ? sv->kt->ms[c] : 0.0;
   return CGP_OK;
 }
 

@@ -336,6 +336,7 @@ typedef struct {
   double admit_ms;           /* host time spent admitting requests                   */
   double retire_ms;          /* host time spent retiring slots and copying results   */
   int64_t retire_passes;     /* snapshot-and-reset passes over the vertices          */
+  double kernel_ms[8];       /* per kernel class when created with profile_kernels   */
 } cgp_server_stats;
 cgp_status cgp_server_get_stats(cgp_server* s, cgp_server_stats* st);
 
