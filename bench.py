@@ -450,6 +450,15 @@ def main():
     if "sssp_push" in ps.kernel_profile:
         ms_k, n_k = ps.kernel_profile["sssp_push"]
         kclass["sssp_push"] = {"ms": ms_k, "launches": n_k, "bytes": bytes_s["sssp_push"]}
+    level_trace = {
+        "bfs": [[p.mode, p.frontier_size, p.frontier_edges, p.new_pairs, p.pull_edges]
+                for p in pb.iteration_profiles],
+        "sssp": [[p.frontier_size, p.frontier_edges, p.sssp_active, p.sssp_pairs, p.improved]
+                 for p in ps.iteration_profiles],
+        "columns": {"bfs": ["mode", "frontier", "frontier_edges", "new_pairs", "pull_edges"],
+                    "sssp": ["frontier", "frontier_edges", "active_bits", "pairs", "improved"]},
+        "kernel_ms": {"bfs": pb.kernel_profile, "sssp": ps.kernel_profile},
+    }
     peak, peak_src = measured_peaks()
     dom = max(kclass, key=lambda k: kclass[k]["ms"]) if kclass else None
     roofline = None
@@ -566,7 +575,8 @@ def main():
                        "tuned": None if args.no_autotune else {
                            "bfs": {"mask_words": opts_b.mask_words, "heavy_degree": opts_b.heavy_degree,
                                    "pull_edge_ratio": opts_b.pull_edge_ratio},
-                           "sssp": {"mask_words": opts_s.mask_words, "heavy_degree": opts_s.heavy_degree},
+                           "sssp": {"mask_words": opts_s.mask_words, "heavy_degree": opts_s.heavy_degree,
+                                    "dense_unroll": opts_s.dense_unroll},
                            "tuning_s": tune_s},
                        "l2": f"inputs larger than L2: CSR {4 * (V + 1 + 2 * g.num_edges) / 2**20:.0f} MiB "
                              f"+ outputs {8 * V * (len(bfs_d) + len(sssp_d)) / 2**30:.1f} GiB "
@@ -583,7 +593,7 @@ def main():
             "one_query": one_query,
             "batched_vs_one_query": (value / world / one_query["gteps"]) if one_query else None,
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-            "serving": serving,
+            "serving": serving, "level_trace": level_trace,
             "cpu_baseline": cpu, "graph_gen_s": gen_s,
         }
         s = json.dumps(line)

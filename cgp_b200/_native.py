@@ -37,7 +37,8 @@ class CgpOptions(Structure):
         ("pull_edge_ratio", c_double), ("profile_iterations", c_int32),
         ("use_cuda_graph", c_int32), ("levels_per_sync", c_int32), ("mask_words", c_int32),
         ("depth_mode", c_int32), ("heavy_degree", c_int32), ("max_queries", c_int32),
-        ("discard_results", c_int32), ("profile_kernels", c_int32), ("reserved", c_int32 * 5),
+        ("discard_results", c_int32), ("profile_kernels", c_int32), ("dense_unroll", c_int32),
+        ("reserved", c_int32 * 4),
         ("stream", c_void_p),
     ]
 

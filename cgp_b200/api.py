@@ -283,6 +283,7 @@ class RunOptions:
     depth_mode: str = "auto"
     heavy_degree: int = 0
     profile_kernels: bool = False
+    dense_unroll: int = 0
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -303,6 +304,7 @@ class RunOptions:
                         "direct": N.DEPTH_DIRECT}[self.depth_mode]
         o.heavy_degree = self.heavy_degree
         o.profile_kernels = int(self.profile_kernels)
+        o.dense_unroll = self.dense_unroll
         o.stream = self.stream or None
         return o
 
@@ -432,7 +434,8 @@ def autotune(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpti
     N.check(N.lib().cgp_autotune(graph.handle, q, len(descs), ctypes.byref(o), reps), "cgp_autotune")
     return dataclasses.replace(options, mask_words=o.mask_words, heavy_degree=o.heavy_degree,
                                pull_edge_ratio=o.pull_edge_ratio,
-                               pull_frontier_ratio=o.pull_frontier_ratio)
+                               pull_frontier_ratio=o.pull_frontier_ratio,
+                               dense_unroll=o.dense_unroll)
 
 
 def run(policy: str, graph: CsrGraph, queries, context=None, options: RunOptions | None = None,

@@ -105,6 +105,16 @@ extern "C" cgp_status cgp_autotune(cgp_graph* graph, const cgp_query* sample, in
       }
     }
   }
+  if (st == CGP_OK && ns > 0) {
+    cgp_options c = best;
+    c.dense_unroll = best.dense_unroll == 2 ? 1 : 2;
+    time_run(graph, sample, n, c, out, 1, &st);
+    float t = time_run(graph, sample, n, c, out, reps, &st);
+    if (st == CGP_OK && t < best_t) {
+      best_t = t;
+      best = c;
+    }
+  }
   if (st == CGP_OK) {
     const int wmax = choose_words(nb + ns + nk, 0);
     for (int w = 1; w < wmax && st == CGP_OK; w <<= 1) {

@@ -259,6 +259,7 @@ struct Grids {
   int heavy;
   int clear;
   int dense;
+  int dense2;
 };
 
 struct LevelLaunch {
@@ -268,7 +269,8 @@ struct LevelLaunch {
   bool has_bfs;
   bool has_sssp;
   bool pull;
-  KernelTimer* kt;  // per-class event timing (non-graph runs only)
+  int dense_unroll;  // edges per step of the dense SSSP kernel (1 or 2)
+  KernelTimer* kt;   // per-class event timing (non-graph runs only)
 };
 
 template <typename K>
@@ -312,7 +314,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
   if (L.has_sssp) {
     if (kt) kt->mark(kClassSsspPush, s);
     k_sssp_push<W, OT, WK><<<t, kBlock, 0, s>>>(L.g, L.G);
-    k_sssp_dense<W, OT, WK><<<L.gr.dense, kBlock, 0, s>>>(L.g, L.G);
+    if (L.dense_unroll == 2)
+      k_sssp_dense<W, OT, WK, 2><<<L.gr.dense2, kBlock, 0, s>>>(L.g, L.G);
+    else
+      k_sssp_dense<W, OT, WK, 1><<<L.gr.dense, kBlock, 0, s>>>(L.g, L.G);
     n += 2;
     if (L.G.n_heavy) {
       k_sssp_push_heavy<W, OT, WK><<<h, kBlock, 0, s>>>(L.g, L.G);
@@ -328,9 +333,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
 
 template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
-  static int tile = 0, heavy = 0, dense = 0;
+  static int tile = 0, heavy = 0, dense = 0, dense2 = 0;
   if (tile == 0) {
-    dense = occupancy_grid(k_sssp_dense<W, OT, WK>, sms);
+    dense = occupancy_grid(k_sssp_dense<W, OT, WK, 1>, sms);
+    dense2 = occupancy_grid(k_sssp_dense<W, OT, WK, 2>, sms);
     int a = occupancy_grid(k_bfs_push<W, OT, DEPTH>, sms);
     int b = occupancy_grid(k_bfs_pull<W, OT, DEPTH>, sms);
     int c = occupancy_grid(k_sssp_push<W, OT, WK>, sms);
@@ -343,6 +349,7 @@ Grids grids_t(int sms) {
   g.heavy = heavy;
   g.clear = sms * 4;
   g.dense = dense;
+  g.dense2 = dense2;
   return g;
 }
 
@@ -509,6 +516,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   int mode = o.traversal_mode;
   if (!g->symmetric && !g->trow.p) mode = CGP_MODE_PUSH;
   L.pull = mode != CGP_MODE_PUSH;
+  L.dense_unroll = o.dense_unroll == 2 ? 2 : 1;
   L.kt = kt;
   if (!o.use_cuda_graph || kt != nullptr) {
     int n = 0;
@@ -519,7 +527,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   L.kt = nullptr;
   auto key = std::make_tuple(spec.W, g->offset_bytes, spec.depth_mode, g->weight_kind,
                              (spec.has_bfs ? 1 : 0) | (spec.has_sssp ? 2 : 0) | (L.pull ? 4 : 0) |
-                                 (o.profile_iterations ? 8 : 0),
+                                 (o.profile_iterations ? 8 : 0) | (L.dense_unroll == 2 ? 16 : 0),
                              levels, spec.Qg, static_cast<int>(L.G.heavy_degree), ws->generation,
                              reinterpret_cast<uint64_t>(L.g.values));
   auto it = ws->graphs.find(key);

@@ -758,7 +758,7 @@ constexpr int kDenseBits = 16;
 // chunk costs one coalesced 128-byte load of the neighbour's row, a compare,
 // and an atomicMin only where it improves; the improved bits of a chunk are
 // combined by a ballot into one atomicOr of the next-frontier word.
-template <int W, typename OT, int WK>
+template <int W, typename OT, int WK, int U>
 __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGraph& G,
                                                  const LevelView& lv, int32_t u,
                                                  const uint64_t (&bits)[W], int64_t eb,
@@ -783,53 +783,67 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
       wl = weight_bits<WK>(G.w, e);
     }
     const int cnt = static_cast<int>(ee - e0 < 32 ? ee - e0 : 32);
-    for (int i = 0; i < cnt; ++i) {
-      const int32_t nb = __shfl_sync(kFull, nl, i);
-      const uint32_t wt = __shfl_sync(kFull, wl, i);
-      uint32_t* row = g.values + static_cast<size_t>(nb) * Qg + lane;
-      // all loads of the active chunks first (independent, in flight together);
-      // improvements are rare, so the atomics and ballots run only when some
-      // lane of the warp has a better candidate for this edge
-      uint32_t cur[2 * W];
+    // U edges per step (1 or 2): U x (active chunks) row loads in flight per warp
+    for (int i = 0; i < cnt; i += U) {
+      const bool two = U == 2 && i + 1 < cnt;
+      const int32_t nb0 = __shfl_sync(kFull, nl, i);
+      const uint32_t wt0 = __shfl_sync(kFull, wl, i);
+      const int32_t nb1 = __shfl_sync(kFull, nl, two ? i + 1 : i);
+      const uint32_t wt1 = __shfl_sync(kFull, wl, two ? i + 1 : i);
+      uint32_t* row0 = g.values + static_cast<size_t>(nb0) * Qg + lane;
+      uint32_t* row1 = g.values + static_cast<size_t>(nb1) * Qg + lane;
+      uint32_t cur0[2 * W], cur1[2 * W];
 #pragma unroll
-      for (int c = 0; c < 2 * W; ++c) cur[c] = act[c] ? row[32 * c] : 0u;
-      uint32_t cand[2 * W];
+      for (int c = 0; c < 2 * W; ++c) {
+        cur0[c] = act[c] ? row0[32 * c] : 0u;
+        cur1[c] = (act[c] && two) ? row1[32 * c] : 0u;
+      }
       bool better = false;
 #pragma unroll
       for (int c = 0; c < 2 * W; ++c) {
-        cand[c] = relax_w<WK>(du[c], wt);
-        better |= act[c] && cand[c] < cur[c];
+        better |= act[c] && relax_w<WK>(du[c], wt0) < cur0[c];
+        better |= act[c] && two && relax_w<WK>(du[c], wt1) < cur1[c];
       }
+      // improvements are rare: atomics and ballots only when some lane of the
+      // warp has a better candidate for one of the two edges
       if (!__any_sync(kFull, better)) continue;
-      bool any = false;
 #pragma unroll
-      for (int c = 0; c < 2 * W; ++c) {
-        if (half[c] == 0) continue;
-        bool imp = false;
-        if (act[c] && cand[c] < cur[c]) imp = cand[c] < atomicMin(row + 32 * c, cand[c]);
-        const unsigned m = __ballot_sync(kFull, imp);
-        if (m) {
-          any = true;
-          if (lane == 0) {
-            const uint64_t bitsw = static_cast<uint64_t>(m) << (32 * (c & 1));
-            atomic_or64(lv.fnext + static_cast<size_t>(nb) * W + (c >> 1), bitsw);
-            uni[c >> 1] |= bitsw;
-            improved += __popc(m);
+      for (int t = 0; t < 2; ++t) {
+        if (t == 1 && !two) break;
+        const int32_t nb = t ? nb1 : nb0;
+        const uint32_t wt = t ? wt1 : wt0;
+        uint32_t* row = t ? row1 : row0;
+        bool any = false;
+#pragma unroll
+        for (int c = 0; c < 2 * W; ++c) {
+          if (half[c] == 0) continue;
+          const uint32_t cand = relax_w<WK>(du[c], wt);
+          bool imp = false;
+          if (act[c] && cand < (t ? cur1[c] : cur0[c])) imp = cand < atomicMin(row + 32 * c, cand);
+          const unsigned m = __ballot_sync(kFull, imp);
+          if (m) {
+            any = true;
+            if (lane == 0) {
+              const uint64_t bitsw = static_cast<uint64_t>(m) << (32 * (c & 1));
+              atomic_or64(lv.fnext + static_cast<size_t>(nb) * W + (c >> 1), bitsw);
+              uni[c >> 1] |= bitsw;
+              improved += __popc(m);
+            }
           }
         }
+        bool app = false;
+        if (any && lane == 0) app = atomicMax(g.stamp + nb, lv.level + 1) < lv.level + 1;
+        warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist, lv.ncount, lv.nedges,
+                    lane);
       }
-      bool app = false;
-      if (any && lane == 0) app = atomicMax(g.stamp + nb, lv.level + 1) < lv.level + 1;
-      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist, lv.ncount, lv.nedges,
-                  lane);
     }
   }
 }
 
 // Dense SSSP vertices of a level, one warp per vertex (the tile kernel
 // queued them), so that this loop gets a register budget of its own.
-template <int W, typename OT, int WK>
-__global__ void __launch_bounds__(kBlock, 4) k_sssp_dense(GroupDev g, DevGraph G) {
+template <int W, typename OT, int WK, int U>
+__global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
   if (ctl->done) return;
   const LevelView lv = level_view(g);
@@ -849,7 +863,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_sssp_dense(GroupDev g, DevGraph G
     load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
 #pragma unroll
     for (int k = 0; k < W; ++k) b[k] &= ctl->sssp_bits[k];
-    sssp_dense_edges<W, OT, WK>(g, G, lv, u, b, beg, end, lane, uni, improved);
+    sssp_dense_edges<W, OT, WK, U>(g, G, lv, u, b, beg, end, lane, uni, improved);
   }
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(improved, &g.ctl->lc.improved, lane);
@@ -1027,7 +1041,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
       const int64_t seg = (ce - cb + nw - 1) / nw;
       const int64_t wb = cb + (threadIdx.x >> 5) * seg;
       const int64_t we = min(ce, wb + seg);
-      sssp_dense_edges<W, OT, WK>(g, G, lv, u, b, wb, we, lane, uni, improved);
+      sssp_dense_edges<W, OT, WK, 1>(g, G, lv, u, b, wb, we, lane, uni, improved);
       __syncthreads();
       continue;
     }

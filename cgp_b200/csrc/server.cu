@@ -126,14 +126,24 @@ __global__ void __launch_bounds__(kBlock) k_retire(GroupDev g, int64_t V, const 
   for (int i = 0; i < n; ++i) any_out |= rq[i].has_out != 0;
   for (int64_t v0 = static_cast<int64_t>(blockIdx.x) * kRetireTile; v0 < V;
        v0 += static_cast<int64_t>(gridDim.x) * kRetireTile) {
-    for (int j = wib; j < kRetireTile; j += kWarpsPerBlock) {
+    // each warp reads its 8 rows' slots first (8 independent loads per lane)
+    constexpr int kPer = kRetireTile / kWarpsPerBlock;
+    uint32_t xs[kPer];
+    RetireReq r{};
+    if (lane < n) r = rq[lane];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int64_t v = v0 + wib + k * kWarpsPerBlock;
+      xs[k] = (lane < n && v < V) ? g.values[static_cast<size_t>(v) * g.Qg + r.slot] : kServeInf;
+    }
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int j = wib + k * kWarpsPerBlock;
       const int64_t v = v0 + j;
       if (v >= V) break;
-      uint32_t* row = g.values + static_cast<size_t>(v) * g.Qg;
       if (lane < n) {
-        const RetireReq r = rq[lane];
-        uint32_t x = row[r.slot];
-        row[r.slot] = kServeInf;
+        g.values[static_cast<size_t>(v) * g.Qg + r.slot] = kServeInf;
+        uint32_t x = xs[k];
         if (x == kServeInf) {
           if (r.kind == 0 || r.kind == 3) x = 0x7fffffffu;
           else if (f32) x = 0x7f800000u;

@@ -105,7 +105,8 @@ typedef struct {
   int32_t max_queries;        /* run_options::max_queries; 0 = unlimited         */
   int32_t discard_results;    /* run_options::discard_results                    */
   int32_t profile_kernels;    /* time kernel classes with CUDA events (slower; no graphs) */
-  int32_t reserved[5];
+  int32_t dense_unroll;       /* edges per step of the dense SSSP kernel: 1 or 2; 0 = 1 */
+  int32_t reserved[4];
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 

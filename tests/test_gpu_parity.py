@@ -354,3 +354,14 @@ def test_autotune_keeps_results_and_caches(rmat_u32):
     for i, d in enumerate(descs):
         exp = oracle.bfs(g, d.source).view(np.uint32) if d.kind == "bfs" else oracle.sssp(g, d.source)
         np.testing.assert_array_equal(r.values[i], exp)
+
+
+@pytest.mark.parametrize("opts", [dict(dense_unroll=2), dict(dense_unroll=1, heavy_degree=64),
+                                  dict(dense_unroll=2, heavy_degree=16, mask_words=8)])
+def test_sssp_execution_knobs_do_not_change_results(rmat_u32, opts):
+    g, graph = rmat_u32
+    src = g.pick_sources(300, seed=23)
+    ref, _ = oracle.batch("sssp", g, src)
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                      cgp.RunOptions(**opts), layout="query")
+    np.testing.assert_array_equal(r.values, ref)
