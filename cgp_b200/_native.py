@@ -62,11 +62,11 @@ class CgpStats(Structure):
 
 
 KERNEL_CLASSES = ["clear", "bfs_push", "bfs_pull", "sssp_push", "level_end", "init", "output",
-                  "wcc"]
+                  "wcc", "sssp_dense", "sssp_heavy", "", ""]
 
 
 class CgpKernelProfile(Structure):
-    _fields_ = [("ms", c_double * 8), ("launches", c_int64 * 8)]
+    _fields_ = [("ms", c_double * 12), ("launches", c_int64 * 12)]
 
 
 class CgpHostCsr(Structure):
@@ -85,7 +85,7 @@ class CgpServerStats(Structure):
     _fields_ = [("slots", c_int32), ("active_slots", c_int32), ("queued", c_int64),
                 ("completed", c_int64), ("levels", c_int64), ("busy_ms", c_double),
                 ("state_bytes", c_int64), ("admit_ms", c_double), ("retire_ms", c_double),
-                ("retire_passes", c_int64), ("kernel_ms", c_double * 8)]
+                ("retire_passes", c_int64), ("kernel_ms", c_double * 12)]
 
 
 # name -> (restype, argtypes)

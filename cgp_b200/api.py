@@ -409,7 +409,7 @@ def run_batch(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpt
         kp = N.CgpKernelProfile()
         N.check(N.lib().cgp_last_kernel_profile(ctypes.byref(kp)))
         kprof = {name: (kp.ms[i], kp.launches[i]) for i, name in enumerate(N.KERNEL_CLASSES)
-                 if kp.launches[i]}
+                 if name and kp.launches[i]}
     return RunResult(values=arr, iterations=stats.iterations, gpu_time_ms=stats.gpu_time_ms,
                      wall_time_ms=stats.wall_time_ms, push_levels=stats.push_levels,
                      pull_levels=stats.pull_levels, groups=stats.groups,
@@ -617,7 +617,7 @@ class Server:
         N.check(N.lib().cgp_server_get_stats(self._h, ctypes.byref(s)), "stats")
         d = {k: getattr(s, k) for k, _ in N.CgpServerStats._fields_ if k != "kernel_ms"}
         d["kernel_ms"] = {name: s.kernel_ms[i] for i, name in enumerate(N.KERNEL_CLASSES)
-                          if s.kernel_ms[i] > 0}
+                          if name and s.kernel_ms[i] > 0}
         return d
 
     def close(self):

@@ -314,12 +314,14 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
   if (L.has_sssp) {
     if (kt) kt->mark(kClassSsspPush, s);
     k_sssp_push<W, OT, WK><<<t, kBlock, 0, s>>>(L.g, L.G);
+    if (kt) kt->mark(kClassSsspDense, s);
     if (L.dense_unroll == 2)
       k_sssp_dense<W, OT, WK, 2><<<L.gr.dense2, kBlock, 0, s>>>(L.g, L.G);
     else
       k_sssp_dense<W, OT, WK, 1><<<L.gr.dense, kBlock, 0, s>>>(L.g, L.G);
     n += 2;
     if (L.G.n_heavy) {
+      if (kt) kt->mark(kClassSsspHeavy, s);
       k_sssp_push_heavy<W, OT, WK><<<h, kBlock, 0, s>>>(L.g, L.G);
       ++n;
     }

@@ -72,11 +72,13 @@ enum KernelClass {
   kClassClear = 0,
   kClassBfsPush,
   kClassBfsPull,
-  kClassSsspPush,
+  kClassSsspPush,   // SSSP tile kernel (few active queries per vertex)
   kClassLevelEnd,
   kClassInit,
   kClassOutput,
   kClassWcc,
+  kClassSsspDense,  // SSSP dense kernel (many active queries per vertex)
+  kClassSsspHeavy,  // SSSP heavy-vertex chunks
   kNumClasses
 };
 

@@ -688,7 +688,7 @@ cgp_status cgp_server_get_stats(cgp_server* sv, cgp_server_stats* st) {
   st->admit_ms = sv->admit_ms;
   st->retire_ms = sv->retire_ms;
   st->retire_passes = sv->retire_passes;
-  for (int c = 0; c < 8; ++c) st->kernel_ms[c] = sv->kt && c < kNumClasses ? sv->kt->ms[c] : 0.0;
+  for (int c = 0; c < 12; ++c) st->kernel_ms[c] = sv->kt && c < kNumClasses ? sv->kt->ms[c] : 0.0;
   return CGP_OK;
 }
 

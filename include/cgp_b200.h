@@ -151,8 +151,9 @@ typedef struct {
 /* Per-kernel-class CUDA-event times of the last cgp_batch_run on this thread
  * that had profile_kernels set. */
 typedef struct {
-  double ms[8];        /* clear, bfs_push, bfs_pull, sssp_push, level_end, init, output, wcc */
-  int64_t launches[8];
+  double ms[12];       /* clear, bfs_push, bfs_pull, sssp_push, level_end, init, output, wcc,
+                          sssp_dense, sssp_heavy */
+  int64_t launches[12];
 } cgp_kernel_profile;
 
 /* Host CSR (generators and loaders); int64 row offsets. */
@@ -337,7 +338,7 @@ typedef struct {
   double admit_ms;           /* host time spent admitting requests                   */
   double retire_ms;          /* host time spent retiring slots and copying results   */
   int64_t retire_passes;     /* snapshot-and-reset passes over the vertices          */
-  double kernel_ms[8];       /* per kernel class when created with profile_kernels   */
+  double kernel_ms[12];      /* per kernel class when created with profile_kernels   */
 } cgp_server_stats;
 cgp_status cgp_server_get_stats(cgp_server* s, cgp_server_stats* st);
 
