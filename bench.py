@@ -57,6 +57,7 @@ def parse_args():
     p.add_argument("--pull-edge-ratio", type=float, default=0.20)
     p.add_argument("--pull-frontier-ratio", type=float, default=0.15)
     p.add_argument("--heavy-degree", type=int, default=0)
+    p.add_argument("--sssp-pull-edge-ratio", type=float, default=0.5)
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--json-out", default="")
     p.add_argument("--serve", action="store_true",
@@ -155,13 +156,15 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- roofline
-def level_bytes(profiles, kind, V, W, ob=4):
+def level_bytes(profiles, kind, V, W, ob=4, qs=0):
     """Algorithmic bytes per kernel class from the per-level counters.
     BFS push: U(2o+Wb+4) + D(4+2Wb) + 4N + Wb U'
     BFS pull: 2 V Wb + P 2o + S(4+Wb) + 4N
-    SSSP push: U(2o+Wb+4) + D(4+4+Wb) + 4 sum(popc) + 8 A + Wb U'"""
+    SSSP push (scatter): U(2o+Wb+4) + D(4+4+Wb) + 4 sum(popc) + 8 A + Wb U'
+    SSSP pull (gather):  2o V + 4 Qs P + S(4+4+Wb) + 4 A + 4 I + Wb U'
+    (A = (edge, active query) pairs, I = improved entries, Qs = SSSP slots)"""
     Wb = 8 * W
-    out = {"bfs_push": 0, "bfs_pull": 0, "sssp_push": 0}
+    out = {"bfs_push": 0, "bfs_pull": 0, "sssp_relax": 0}
     for p in profiles:
         U, D, N, Un = p.frontier_size, p.frontier_edges, p.new_pairs, p.next_size
         if kind == "bfs":
@@ -170,9 +173,13 @@ def level_bytes(profiles, kind, V, W, ob=4):
             else:
                 out["bfs_pull"] += (2 * V * Wb + p.pull_vertices * 2 * ob
                                     + p.pull_edges * (4 + Wb) + 4 * N)
+        elif p.sssp_mode == "push":
+            out["sssp_relax"] += (U * (2 * ob + Wb + 4) + D * (4 + 4 + Wb) + 4 * p.sssp_active
+                                  + 8 * p.sssp_pairs + Wb * Un)
         else:
-            out["sssp_push"] += (U * (2 * ob + Wb + 4) + D * (4 + 4 + Wb) + 4 * p.sssp_active
-                                 + 8 * p.sssp_pairs + Wb * Un)
+            out["sssp_relax"] += (2 * ob * V + 4 * qs * p.sssp_pull_vertices
+                                  + p.sssp_pull_edges * (4 + 4 + Wb) + 4 * p.sssp_pairs
+                                  + 4 * p.improved + Wb * Un)
     return out
 
 
@@ -380,7 +387,8 @@ def main():
     out_s = torch.empty((V, len(sssp_d)), dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
     tuning = dict(traversal_mode=args.mode, pull_edge_ratio=args.pull_edge_ratio,
-                  pull_frontier_ratio=args.pull_frontier_ratio, heavy_degree=args.heavy_degree)
+                  pull_frontier_ratio=args.pull_frontier_ratio, heavy_degree=args.heavy_degree,
+                  sssp_pull_edge_ratio=args.sssp_pull_edge_ratio)
     opts = cgp.RunOptions(stream=stream.cuda_stream, **tuning)
 
     empty = cgp.RunResult(values=None, iterations=0, gpu_time_ms=0.0, wall_time_ms=0.0)
@@ -441,25 +449,27 @@ def main():
           if sssp_d else empty)
     W = pb.mask_words or ps.mask_words
     bytes_b = level_bytes(pb.iteration_profiles, "bfs", V, W)
-    bytes_s = level_bytes(ps.iteration_profiles, "sssp", V, ps.mask_words)
+    bytes_s = level_bytes(ps.iteration_profiles, "sssp", V, ps.mask_words, qs=len(sssp_d))
     kclass = {}
     for name in ("bfs_push", "bfs_pull"):
         if name in pb.kernel_profile:
             ms_k, n_k = pb.kernel_profile[name]
             kclass[name] = {"ms": ms_k, "launches": n_k, "bytes": bytes_b[name]}
     if "sssp_push" in ps.kernel_profile:
-        # the SSSP level = tile + dense + heavy kernels; bytes are counted per level
+        # one SSSP level = scatter (tile + dense + heavy) or gather (light +
+        # heavy) kernels; bytes are counted per level
         ms_k = sum(ps.kernel_profile.get(k, (0.0, 0))[0]
-                   for k in ("sssp_push", "sssp_dense", "sssp_heavy"))
+                   for k in ("sssp_push", "sssp_dense", "sssp_heavy", "sssp_pull"))
         n_k = ps.kernel_profile["sssp_push"][1]
-        kclass["sssp_push"] = {"ms": ms_k, "launches": n_k, "bytes": bytes_s["sssp_push"]}
+        kclass["sssp_relax"] = {"ms": ms_k, "launches": n_k, "bytes": bytes_s["sssp_relax"]}
     level_trace = {
         "bfs": [[p.mode, p.frontier_size, p.frontier_edges, p.new_pairs, p.pull_edges]
                 for p in pb.iteration_profiles],
-        "sssp": [[p.frontier_size, p.frontier_edges, p.sssp_active, p.sssp_pairs, p.improved]
-                 for p in ps.iteration_profiles],
+        "sssp": [[p.sssp_mode, p.frontier_size, p.frontier_edges, p.sssp_active, p.sssp_pairs,
+                  p.improved, p.sssp_pull_edges] for p in ps.iteration_profiles],
         "columns": {"bfs": ["mode", "frontier", "frontier_edges", "new_pairs", "pull_edges"],
-                    "sssp": ["frontier", "frontier_edges", "active_bits", "pairs", "improved"]},
+                    "sssp": ["mode", "frontier", "frontier_edges", "active_bits", "pairs",
+                             "improved", "pull_edges"]},
         "kernel_ms": {"bfs": pb.kernel_profile, "sssp": ps.kernel_profile},
     }
     peak, peak_src = measured_peaks()
@@ -579,7 +589,8 @@ def main():
                            "bfs": {"mask_words": opts_b.mask_words, "heavy_degree": opts_b.heavy_degree,
                                    "pull_edge_ratio": opts_b.pull_edge_ratio},
                            "sssp": {"mask_words": opts_s.mask_words, "heavy_degree": opts_s.heavy_degree,
-                                    "dense_unroll": opts_s.dense_unroll},
+                                    "dense_unroll": opts_s.dense_unroll,
+                                    "sssp_pull_edge_ratio": opts_s.sssp_pull_edge_ratio},
                            "tuning_s": tune_s},
                        "l2": f"inputs larger than L2: CSR {4 * (V + 1 + 2 * g.num_edges) / 2**20:.0f} MiB "
                              f"+ outputs {8 * V * (len(bfs_d) + len(sssp_d)) / 2**30:.1f} GiB "

@@ -38,7 +38,7 @@ class CgpOptions(Structure):
         ("use_cuda_graph", c_int32), ("levels_per_sync", c_int32), ("mask_words", c_int32),
         ("depth_mode", c_int32), ("heavy_degree", c_int32), ("max_queries", c_int32),
         ("discard_results", c_int32), ("profile_kernels", c_int32), ("dense_unroll", c_int32),
-        ("reserved", c_int32 * 4),
+        ("sssp_pull_edge_ratio", c_double), ("reserved", c_int32 * 2),
         ("stream", c_void_p),
     ]
 
@@ -48,7 +48,9 @@ class CgpLevelProfile(Structure):
                 ("frontier_edges", c_uint64), ("next_size", c_uint64),
                 ("query_convergence_mask", c_uint64), ("new_pairs", c_uint64),
                 ("pull_vertices", c_uint64), ("pull_edges", c_uint64), ("sssp_pairs", c_uint64),
-                ("sssp_active", c_uint64), ("improved", c_uint64)]
+                ("sssp_active", c_uint64), ("improved", c_uint64),
+                ("sssp_pull_vertices", c_uint64), ("sssp_pull_edges", c_uint64),
+                ("sssp_mode", c_int32), ("reserved", c_int32)]
 
 
 class CgpStats(Structure):
@@ -58,11 +60,12 @@ class CgpStats(Structure):
                 ("device_status", c_uint64), ("mask_words", c_int32), ("depth_mode", c_int32),
                 ("kernel_launches", c_uint64), ("new_pairs", c_uint64), ("pull_vertices", c_uint64),
                 ("pull_edges", c_uint64), ("sssp_pairs", c_uint64), ("sssp_active", c_uint64),
-                ("improved", c_uint64)]
+                ("improved", c_uint64), ("sssp_pull_vertices", c_uint64),
+                ("sssp_pull_edges", c_uint64)]
 
 
 KERNEL_CLASSES = ["clear", "bfs_push", "bfs_pull", "sssp_push", "level_end", "init", "output",
-                  "wcc", "sssp_dense", "sssp_heavy", "", ""]
+                  "wcc", "sssp_dense", "sssp_heavy", "sssp_pull", ""]
 
 
 class CgpKernelProfile(Structure):

@@ -284,6 +284,7 @@ class RunOptions:
     heavy_degree: int = 0
     profile_kernels: bool = False
     dense_unroll: int = 0
+    sssp_pull_edge_ratio: float = 0.5
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -305,6 +306,7 @@ class RunOptions:
         o.heavy_degree = self.heavy_degree
         o.profile_kernels = int(self.profile_kernels)
         o.dense_unroll = self.dense_unroll
+        o.sssp_pull_edge_ratio = self.sssp_pull_edge_ratio
         o.stream = self.stream or None
         return o
 
@@ -324,6 +326,9 @@ class IterationProfile:
     sssp_pairs: int = 0
     sssp_active: int = 0
     improved: int = 0
+    sssp_pull_vertices: int = 0
+    sssp_pull_edges: int = 0
+    sssp_mode: str = "push"
 
 
 @dataclass
@@ -402,7 +407,8 @@ def run_batch(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpt
         profiles = [IterationProfile(p.iteration, "pull" if p.mode else "push", p.frontier_size,
                                      p.frontier_edges, p.next_size, p.query_convergence_mask,
                                      p.new_pairs, p.pull_vertices, p.pull_edges, p.sssp_pairs,
-                                     p.sssp_active, p.improved)
+                                     p.sssp_active, p.improved, p.sssp_pull_vertices,
+                                     p.sssp_pull_edges, "pull" if p.sssp_mode else "push")
                     for p in buf[:cnt.value]]
     kprof = {}
     if options.profile_kernels:
@@ -419,7 +425,9 @@ def run_batch(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpt
                      effective_query_dim=len(descs), kernel_launches=stats.kernel_launches,
                      counters={k: getattr(stats, k) for k in ("new_pairs", "pull_vertices",
                                                               "pull_edges", "sssp_pairs",
-                                                              "sssp_active", "improved")},
+                                                              "sssp_active", "improved",
+                                                              "sssp_pull_vertices",
+                                                              "sssp_pull_edges")},
                      kernel_profile=kprof, iteration_profiles=profiles, options=options)
 
 
@@ -435,7 +443,8 @@ def autotune(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpti
     return dataclasses.replace(options, mask_words=o.mask_words, heavy_degree=o.heavy_degree,
                                pull_edge_ratio=o.pull_edge_ratio,
                                pull_frontier_ratio=o.pull_frontier_ratio,
-                               dense_unroll=o.dense_unroll)
+                               dense_unroll=o.dense_unroll,
+                               sssp_pull_edge_ratio=o.sssp_pull_edge_ratio)
 
 
 def run(policy: str, graph: CsrGraph, queries, context=None, options: RunOptions | None = None,

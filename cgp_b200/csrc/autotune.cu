@@ -1,7 +1,8 @@
 // Autotuner: picks the bitmask width (queries per traversal group), the
 // heavy-vertex threshold (degree above which an adjacency list is split into
-// CTA work items) and the push->pull switch threshold for one graph and one
-// query mix, by timing short runs of a representative batch.
+// CTA work items), the BFS push->pull and SSSP scatter->gather switch
+// thresholds and the dense SSSP step width for one graph and one query mix,
+// by timing short runs of a representative batch.
 //
 // The reference fixes these: 64-bit masks (puercgp/include/puercgp/core/types.hxx:24),
 // degree buckets at 8/512 (frontier_engine.hxx:945-946) and pull ratios
@@ -97,6 +98,20 @@ extern "C" cgp_status cgp_autotune(cgp_graph* graph, const cgp_query* sample, in
       cgp_options c = best;
       c.heavy_degree = h;
       time_run(graph, sample, n, c, out, 1, &st);  // builds the heavy table once
+      float t = time_run(graph, sample, n, c, out, reps, &st);
+      if (st != CGP_OK) break;
+      if (t < best_t) {
+        best_t = t;
+        best = c;
+      }
+    }
+  }
+  if (st == CGP_OK && ns > 0 && best.traversal_mode == CGP_MODE_HYBRID) {
+    // SSSP gather threshold (<= 0: scatter only)
+    for (double r : {0.0, 0.25, 0.75}) {
+      cgp_options c = best;
+      c.sssp_pull_edge_ratio = r;
+      time_run(graph, sample, n, c, out, 1, &st);
       float t = time_run(graph, sample, n, c, out, reps, &st);
       if (st != CGP_OK) break;
       if (t < best_t) {

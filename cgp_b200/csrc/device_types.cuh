@@ -38,6 +38,10 @@ struct LevelProfile {
   unsigned long long sssp_pairs;    // A_l: (edge, active query) relaxations attempted
   unsigned long long sssp_active;   // sum over frontier vertices of active SSSP bits
   unsigned long long improved;      // SSSP (query, vertex) improvements
+  unsigned long long spull_vertices; // vertices an SSSP gather level scanned
+  unsigned long long spull_edges;    // in-edges an SSSP gather level scanned
+  int32_t sdir;                     // SSSP direction of the level (push / gather)
+  int32_t reserved;
 };
 
 // Per-level work counters (reset by the level-end kernel).
@@ -48,6 +52,8 @@ struct LevelCounters {
   unsigned long long sssp_pairs;
   unsigned long long sssp_active;
   unsigned long long improved;
+  unsigned long long spull_vertices;
+  unsigned long long spull_edges;
 };
 
 // Control block of one traversal group (device memory).
@@ -62,7 +68,9 @@ struct LevelCtl {
   uint64_t bfs_bits[kMaxW];     // slots with visited-mask semantics (BFS, k-hop)
   uint64_t sssp_bits[kMaxW];    // slots with min-reduce semantics (SSSP)
   int32_t level;
-  int32_t dir;
+  int32_t dir;                  // BFS direction of the current level
+  int32_t sdir;                 // SSSP direction: push (scatter) or pull (gather)
+  int32_t sssp_gather;          // gather kernels are launched (pull CSR + weights exist)
   int32_t done;
   uint32_t status;
   int32_t forced_dir;           // -1: decide; else direction of the next level
@@ -75,6 +83,7 @@ struct LevelCtl {
   int32_t profile_cap;
   unsigned long long pull_vertex_threshold;
   unsigned long long pull_edge_threshold;
+  unsigned long long sssp_pull_edge_threshold;  // gather when frontier edges reach it
   unsigned long long dense_count;  // SSSP vertices queued for the dense kernel this level
   LevelCounters lc;                // counters of the current level
   LevelCounters total;             // sums over all levels
@@ -94,6 +103,7 @@ struct DevGraph {
   const void* w;
   const void* prow;      // CSR used by pull (the transpose for directed graphs)
   const int32_t* pcol;
+  const void* pw;        // weights aligned with pcol: pw[e] = weight of pcol[e] -> v
   int64_t V;
   int64_t E;
   const int32_t* heavy;             // vertices with out-degree > heavy_degree

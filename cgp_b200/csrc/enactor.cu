@@ -105,7 +105,7 @@ cgp_status cgp_advance_filter_level(cgp_enactor* e, int32_t direction, int64_t* 
       if (next_size) *next_size = 0;
       return CGP_OK;
     }
-    if (direction == CGP_MODE_PULL && !e->g->symmetric && !e->g->trow.p)
+    if (direction == CGP_MODE_PULL && !e->g->can_gather())
       return set_error(CGP_ERR_INVALID_ARG, "pull needs a symmetric graph or its transpose");
     if (direction != CGP_MODE_HYBRID && e->spec.has_bfs) {
       int32_t dir = direction == CGP_MODE_PULL ? kDirPull : kDirPush;

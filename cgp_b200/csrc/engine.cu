@@ -117,6 +117,7 @@ DevGraph GraphImpl::dev_graph(int64_t h) {
   d.w = w.p;
   d.prow = pull_row();
   d.pcol = pull_col();
+  d.pw = pull_w();
   d.V = V;
   d.E = E;
   d.heavy = hp.heavy.vertices.as<int32_t>();
@@ -172,7 +173,7 @@ const HeavyPair& GraphImpl::heavy_for(int64_t h) {
     std::lock_guard<std::mutex> hl(g_host_mu);
     HostCsr& hc = g_host[this];
     build_heavy(hc.row, V, h, hp->heavy);
-    build_heavy(symmetric ? hc.row : hc.trow, V, h, hp->pheavy);
+    build_heavy(hc.trow.empty() ? hc.row : hc.trow, V, h, hp->pheavy);
   }
   return *heavy_cache.emplace(h, std::move(hp)).first->second;
 }
@@ -260,6 +261,8 @@ struct Grids {
   int clear;
   int dense;
   int dense2;
+  int gather;
+  int gather_heavy;
 };
 
 struct LevelLaunch {
@@ -269,6 +272,7 @@ struct LevelLaunch {
   bool has_bfs;
   bool has_sssp;
   bool pull;
+  bool spull;        // SSSP gather kernels are part of the level
   int dense_unroll;  // edges per step of the dense SSSP kernel (1 or 2)
   KernelTimer* kt;   // per-class event timing (non-graph runs only)
 };
@@ -325,6 +329,15 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
       k_sssp_push_heavy<W, OT, WK><<<h, kBlock, 0, s>>>(L.g, L.G);
       ++n;
     }
+    if (L.spull) {
+      if (kt) kt->mark(kClassSsspPull, s);
+      k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
+      ++n;
+      if (L.G.n_pheavy) {
+        k_sssp_pull_heavy<W, OT, WK><<<L.gr.gather_heavy, kBlock, 0, s>>>(L.g, L.G);
+        ++n;
+      }
+    }
   }
   if (kt) kt->mark(kClassLevelEnd, s);
   k_level_end<W><<<1, 32, 0, s>>>(L.g);
@@ -335,8 +348,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
 
 template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
-  static int tile = 0, heavy = 0, dense = 0, dense2 = 0;
+  static int tile = 0, heavy = 0, dense = 0, dense2 = 0, gather = 0, gather_heavy = 0;
   if (tile == 0) {
+    gather = occupancy_grid(k_sssp_pull<W, OT, WK>, sms);
+    gather_heavy = occupancy_grid(k_sssp_pull_heavy<W, OT, WK>, sms);
     dense = occupancy_grid(k_sssp_dense<W, OT, WK, 1>, sms);
     dense2 = occupancy_grid(k_sssp_dense<W, OT, WK, 2>, sms);
     int a = occupancy_grid(k_bfs_push<W, OT, DEPTH>, sms);
@@ -352,6 +367,8 @@ Grids grids_t(int sms) {
   g.clear = sms * 4;
   g.dense = dense;
   g.dense2 = dense2;
+  g.gather = gather;
+  g.gather_heavy = gather_heavy;
   return g;
 }
 
@@ -422,6 +439,13 @@ GroupDev group_dev(Workspace* ws, const GroupSpec& spec, bool profiles) {
 
 constexpr int kProfileCap = 1 << 16;
 
+// SSSP levels may gather (pull) when the pull CSR exists and the options
+// allow it: always in pull mode, by frontier edges in hybrid mode.
+bool sssp_gather_on(const GraphImpl* g, const cgp_options& o) {
+  if (!g->can_gather() || o.traversal_mode == CGP_MODE_PUSH) return false;
+  return o.traversal_mode == CGP_MODE_PULL || o.sssp_pull_edge_ratio > 0;
+}
+
 }  // namespace
 
 void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
@@ -478,7 +502,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   c.halt_level = -1;
   c.max_iterations = o.max_iterations;
   int mode = o.traversal_mode;
-  if (!g->symmetric && !g->trow.p) mode = CGP_MODE_PUSH;
+  if (!g->can_gather()) mode = CGP_MODE_PUSH;
   c.mode = mode;
   c.num_planes = spec.depth_mode == kDepthPlanes ? kInitialPlanes : 0;
   c.profile_cap = o.profile_iterations ? kProfileCap : 0;
@@ -486,6 +510,9 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
       std::max(1.0, o.pull_frontier_ratio * static_cast<double>(V)));
   c.pull_edge_threshold = static_cast<unsigned long long>(
       std::max(1.0, o.pull_edge_ratio * static_cast<double>(g->E)));
+  c.sssp_gather = sssp_gather_on(g, o) ? 1 : 0;
+  c.sssp_pull_edge_threshold = static_cast<unsigned long long>(
+      std::max(1.0, o.sssp_pull_edge_ratio * static_cast<double>(g->E)));
   ck(cudaMemcpyAsync(ws->ctl.p, &c, sizeof(LevelCtl), cudaMemcpyHostToDevice, s), "upload ctl");
 
   const uint32_t sssp_inf = g->weight_kind == CGP_WEIGHT_F32 ? 0x7f800000u : 0xffffffffu;
@@ -516,8 +543,9 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   L.has_bfs = spec.has_bfs;
   L.has_sssp = spec.has_sssp;
   int mode = o.traversal_mode;
-  if (!g->symmetric && !g->trow.p) mode = CGP_MODE_PUSH;
+  if (!g->can_gather()) mode = CGP_MODE_PUSH;
   L.pull = mode != CGP_MODE_PUSH;
+  L.spull = spec.has_sssp && sssp_gather_on(g, o);
   L.dense_unroll = o.dense_unroll == 2 ? 2 : 1;
   L.kt = kt;
   if (!o.use_cuda_graph || kt != nullptr) {
@@ -529,7 +557,8 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   L.kt = nullptr;
   auto key = std::make_tuple(spec.W, g->offset_bytes, spec.depth_mode, g->weight_kind,
                              (spec.has_bfs ? 1 : 0) | (spec.has_sssp ? 2 : 0) | (L.pull ? 4 : 0) |
-                                 (o.profile_iterations ? 8 : 0) | (L.dense_unroll == 2 ? 16 : 0),
+                                 (o.profile_iterations ? 8 : 0) | (L.dense_unroll == 2 ? 16 : 0) |
+                                 (L.spull ? 32 : 0),
                              levels, spec.Qg, static_cast<int>(L.G.heavy_degree), ws->generation,
                              reinterpret_cast<uint64_t>(L.g.values));
   auto it = ws->graphs.find(key);
@@ -743,26 +772,57 @@ cgp_status cgp_graph_create(const void* row_offsets, int32_t offset_bytes,
                       on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice), "upload weights");
     }
     G.symmetric = (flags & CGP_GRAPH_SYMMETRIC) != 0 || csr_is_symmetric(hrow, hcol.data(), num_vertices);
+    // Pull CSR.  A directed graph needs its transpose.  A symmetric one can be
+    // pulled over directly, except that an SSSP gather also needs, per entry
+    // (v, u), the weight of u -> v: the transpose (counting sort by
+    // destination, sources ascending) gives it, and when its columns equal
+    // the CSR's (sorted lists, no multi-edge mismatch) only the weights are
+    // kept, or nothing when they equal w.
     std::vector<int64_t> trow;
-    if (!G.symmetric) {
-      // in-edge CSR (counting sort by destination) for pull levels
+    const bool weighted = weight_kind != CGP_WEIGHT_NONE;
+    if (!G.symmetric || weighted) {
+      std::vector<uint32_t> hw;
+      if (weighted) {
+        hw.resize(num_edges);
+        if (num_edges > 0)
+          ck(cudaMemcpy(hw.data(), weights, num_edges * 4, kind), "read weights");
+      }
       trow.assign(num_vertices + 1, 0);
       for (int64_t e = 0; e < num_edges; ++e) trow[hcol[e] + 1]++;
       for (int64_t v = 0; v < num_vertices; ++v) trow[v + 1] += trow[v];
       std::vector<int64_t> cur(trow.begin(), trow.end() - 1);
       std::vector<int32_t> tcol(num_edges);
+      std::vector<uint32_t> tw(weighted ? num_edges : 0);
       for (int64_t u = 0; u < num_vertices; ++u)
-        for (int64_t e = hrow[u]; e < hrow[u + 1]; ++e) tcol[cur[hcol[e]]++] = static_cast<int32_t>(u);
-      G.trow.ensure((num_vertices + 1) * G.offset_bytes);
-      if (off64) {
-        ck(cudaMemcpy(G.trow.p, trow.data(), (num_vertices + 1) * 8, cudaMemcpyHostToDevice), "upload t-offsets");
+        for (int64_t e = hrow[u]; e < hrow[u + 1]; ++e) {
+          const int64_t p = cur[hcol[e]]++;
+          tcol[p] = static_cast<int32_t>(u);
+          if (weighted) tw[p] = hw[e];
+        }
+      const bool aligned = G.symmetric && trow == hrow && tcol == hcol;
+      if (aligned) {
+        trow.clear();
+        if (tw != hw) {
+          G.tw.ensure(std::max<int64_t>(num_edges, 1) * 4);
+          ck(cudaMemcpy(G.tw.p, tw.data(), num_edges * 4, cudaMemcpyHostToDevice), "upload t-weights");
+        }
       } else {
-        std::vector<int32_t> r32(trow.begin(), trow.end());
-        ck(cudaMemcpy(G.trow.p, r32.data(), (num_vertices + 1) * 4, cudaMemcpyHostToDevice), "upload t-offsets");
+        G.trow.ensure((num_vertices + 1) * G.offset_bytes);
+        if (off64) {
+          ck(cudaMemcpy(G.trow.p, trow.data(), (num_vertices + 1) * 8, cudaMemcpyHostToDevice), "upload t-offsets");
+        } else {
+          std::vector<int32_t> r32(trow.begin(), trow.end());
+          ck(cudaMemcpy(G.trow.p, r32.data(), (num_vertices + 1) * 4, cudaMemcpyHostToDevice), "upload t-offsets");
+        }
+        G.tcol.ensure(std::max<int64_t>(num_edges, 1) * 4);
+        if (num_edges > 0)
+          ck(cudaMemcpy(G.tcol.p, tcol.data(), num_edges * 4, cudaMemcpyHostToDevice), "upload t-columns");
+        if (weighted) {
+          G.tw.ensure(std::max<int64_t>(num_edges, 1) * 4);
+          if (num_edges > 0)
+            ck(cudaMemcpy(G.tw.p, tw.data(), num_edges * 4, cudaMemcpyHostToDevice), "upload t-weights");
+        }
       }
-      G.tcol.ensure(std::max<int64_t>(num_edges, 1) * 4);
-      if (num_edges > 0)
-        ck(cudaMemcpy(G.tcol.p, tcol.data(), num_edges * 4, cudaMemcpyHostToDevice), "upload t-columns");
     }
     {
       std::lock_guard<std::mutex> lk(g_host_mu);
@@ -818,6 +878,10 @@ cgp_status cgp_last_profiles(cgp_level_profile* out, int32_t cap, int32_t* count
       out[i].sssp_pairs = t_profiles[i].sssp_pairs;
       out[i].sssp_active = t_profiles[i].sssp_active;
       out[i].improved = t_profiles[i].improved;
+      out[i].sssp_pull_vertices = t_profiles[i].spull_vertices;
+      out[i].sssp_pull_edges = t_profiles[i].spull_edges;
+      out[i].sssp_mode = t_profiles[i].sdir;
+      out[i].reserved = 0;
     }
   }
   return CGP_OK;
@@ -941,6 +1005,8 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
       total.counters.sssp_pairs += r.counters.sssp_pairs;
       total.counters.sssp_active += r.counters.sssp_active;
       total.counters.improved += r.counters.improved;
+      total.counters.spull_vertices += r.counters.spull_vertices;
+      total.counters.spull_edges += r.counters.spull_edges;
       if (groups == 0) {
         W0 = spec.W;
         depth0 = spec.depth_mode;
@@ -985,6 +1051,8 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
       stats->sssp_pairs = total.counters.sssp_pairs;
       stats->sssp_active = total.counters.sssp_active;
       stats->improved = total.counters.improved;
+      stats->sssp_pull_vertices = total.counters.spull_vertices;
+      stats->sssp_pull_edges = total.counters.spull_edges;
     }
     g->release(std::move(ws));
     return CGP_OK;

@@ -79,6 +79,7 @@ enum KernelClass {
   kClassWcc,
   kClassSsspDense,  // SSSP dense kernel (many active queries per vertex)
   kClassSsspHeavy,  // SSSP heavy-vertex chunks
+  kClassSsspPull,   // SSSP gather levels (light and heavy vertices)
   kNumClasses
 };
 
@@ -125,14 +126,23 @@ struct GraphImpl {
   int weight_kind = CGP_WEIGHT_NONE;
   bool symmetric = false;
   DevBuf row, col, w;      // traversal CSR
-  DevBuf trow, tcol;       // transpose (in-edges) for pull on directed graphs
+  DevBuf trow, tcol;       // in-edge CSR for pull when the CSR itself cannot serve
+  DevBuf tw;               // weights aligned with the pull CSR when they differ from w
   std::mutex mu;
   std::mutex heavy_mu;
   std::map<int64_t, std::unique_ptr<HeavyPair>> heavy_cache;  // built once per threshold
   std::vector<std::unique_ptr<Workspace>> pool;  // idle workspaces
 
-  const void* pull_row() const { return symmetric ? row.p : trow.p; }
-  const int32_t* pull_col() const { return symmetric ? col.as<int32_t>() : tcol.as<int32_t>(); }
+  // Pull CSR: the CSR itself when it lists every vertex's in-edges in the
+  // order of the transpose (symmetric, sorted), else the stored transpose.
+  const void* pull_row() const { return trow.p ? trow.p : (symmetric ? row.p : nullptr); }
+  const int32_t* pull_col() const {
+    return trow.p ? tcol.as<int32_t>() : (symmetric ? col.as<int32_t>() : nullptr);
+  }
+  // pw[e] = weight of the edge pull_col()[e] -> v (the reverse edge's weight).
+  const void* pull_w() const { return tw.p ? tw.p : w.p; }
+  // SSSP gather levels need the pull CSR (and its weights on weighted graphs).
+  bool can_gather() const { return pull_row() != nullptr; }
   // Heavy tables for threshold h (built on first use, then kept).
   const HeavyPair& heavy_for(int64_t h);
   dev::DevGraph dev_graph(int64_t h);

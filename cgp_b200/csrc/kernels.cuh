@@ -845,7 +845,7 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
 template <int W, typename OT, int WK, int U>
 __global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done) return;
+  if (ctl->done || ctl->sdir != kDirPush) return;
   const LevelView lv = level_view(g);
   const unsigned long long n = ctl->dense_count;
   const int lane = threadIdx.x & 31;
@@ -875,7 +875,7 @@ __global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDe
 template <int W, typename OT, int WK>
 __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done) return;
+  if (ctl->done || ctl->sdir != kDirPush) return;
   const LevelView lv = level_view(g);
   const unsigned long long n = ctl->count[lv.par];
   uint64_t sel[W];
@@ -984,7 +984,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
 template <int W, typename OT, int WK>
 __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done || G.n_heavy == 0) return;
+  if (ctl->done || ctl->sdir != kDirPush || G.n_heavy == 0) return;
   const LevelView lv = level_view(g);
   __shared__ int32_t s_h;
   __shared__ int32_t s_k;
@@ -1080,6 +1080,250 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
   warp_add(improved, &g.ctl->lc.improved, lane);
 }
 
+
+// ------------------------------------------------------------ SSSP gather
+// Dense SSSP levels (most vertices in the frontier for many queries) run as a
+// gather instead of a scatter: the warp that owns vertex v takes the minimum
+// of dist[u][q] + w(u, v) over v's in-edges for all its SSSP slots at once,
+// then writes the improved entries of v's row with plain stores.  No
+// distance atomics, no per-(edge, query) frontier atomics: the improved bits
+// of a 32-slot chunk come from one ballot.  Lane j owns slot 32c + j of
+// chunk c; the sources' rows are read for every SSSP slot of the chunk (an
+// entry that is not in the frontier relaxes to a value that cannot improve
+// v, or to one that another relaxation would produce anyway), so per edge the
+// warp issues 2W coalesced 128-byte loads and no data-dependent branches.
+// Several in-edges are in flight per warp (GatherSteps) to cover latency.
+
+// Relaxation of a stored value `du` over an edge with raw weight bits.  The
+// unreached markers (0xffffffff; +inf for f32) never improve anything.
+template <int WK>
+__device__ __forceinline__ uint32_t gather_relax(uint32_t du, uint32_t wbits) {
+  if constexpr (WK == kWeightF32) {
+    return du >= 0x7f800000u
+               ? 0xffffffffu
+               : __float_as_uint(__fadd_rn(__uint_as_float(du), __uint_as_float(wbits)));
+  } else {
+    const uint32_t wt = (WK == kWeightU32) ? wbits : 1u;
+    return min(du, ~wt) + wt;  // saturates at 0xffffffff
+  }
+}
+
+// In-edges gathered together per warp step: 2W x steps row loads per lane.
+template <int W>
+struct GatherSteps {
+  static constexpr int value = W >= 16 ? 1 : (W >= 8 ? 2 : (W >= 4 ? 4 : 8));
+};
+
+// Bit c of the result: this lane's slot of chunk c is an SSSP slot.
+template <int W>
+__device__ __forceinline__ uint32_t lane_sssp_chunks(const LevelCtl* ctl, int lane) {
+  uint32_t sel = 0;
+#pragma unroll
+  for (int c = 0; c < 2 * W; ++c)
+    sel |= static_cast<uint32_t>((ctl->sssp_bits[c >> 1] >> (32 * (c & 1) + lane)) & 1ULL) << c;
+  return sel;
+}
+
+// min-accumulates relaxations over in-edges [eb, ee) of the pull CSR into
+// best[c] (lane's slot of chunk c).  Edges whose source has no SSSP frontier
+// bit are skipped by a ballot.  All lanes call.
+template <int W, int WK>
+__device__ __forceinline__ void gather_edges(const GroupDev& g, const DevGraph& G,
+                                             const LevelView& lv, const uint64_t* sb,
+                                             uint32_t lsel, int64_t eb, int64_t ee, int lane,
+                                             uint32_t (&best)[2 * W],
+                                             unsigned long long& pairs,
+                                             unsigned& scanned) {
+  constexpr int C = 2 * W;
+  constexpr int S = GatherSteps<W>::value;
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  for (int64_t e0 = eb; e0 < ee; e0 += 32) {
+    const int64_t e = e0 + lane;
+    int32_t u = 0;
+    uint32_t wb = 0;
+    int k = 0;
+    if (e < ee) {
+      u = G.pcol[e];
+      wb = weight_bits<WK>(G.pw, e);
+      uint64_t m[W];
+      load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
+#pragma unroll
+      for (int i = 0; i < W; ++i) k += __popcll(m[i] & sb[i]);
+      ++scanned;
+    }
+    pairs += static_cast<unsigned long long>(k);
+    unsigned live = __ballot_sync(kFull, k > 0);
+    while (live) {
+      int32_t us[S];
+      uint32_t ws[S];
+      bool ok[S];
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        ok[t] = live != 0;
+        const int j = (__ffs(live) - 1) & 31;
+        live &= live - 1;
+        us[t] = __shfl_sync(kFull, u, j);
+        ws[t] = __shfl_sync(kFull, wb, j);
+      }
+      uint32_t cur[S][C];
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        const uint32_t* row = g.values + static_cast<size_t>(us[t]) * Qg + lane;
+#pragma unroll
+        for (int c = 0; c < C; ++c)
+          cur[t][c] = (ok[t] && ((lsel >> c) & 1u)) ? __ldcg(row + 32 * c) : 0xffffffffu;
+      }
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) best[c] = min(best[c], gather_relax<WK>(cur[t][c], ws[t]));
+      }
+    }
+  }
+}
+
+// Gather level, vertices of in-degree <= heavy_degree: one warp per vertex.
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 2)) k_sssp_pull(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->sdir != kDirPull) return;
+  const LevelView lv = level_view(g);
+  constexpr int C = 2 * W;
+  const int lane = threadIdx.x & 31;
+  const uint64_t* sb = ctl->sssp_bits;
+  const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
+  const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long improved = 0, pairs = 0;
+  unsigned scanned = 0, verts = 0;
+  for (unsigned long long vv = gw; vv < static_cast<unsigned long long>(G.V); vv += nwarps) {
+    const int32_t v = static_cast<int32_t>(vv);
+    const int64_t beg = row_at<OT>(G.prow, v);
+    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+    if (end == beg || end - beg > G.heavy_degree) continue;
+    ++verts;
+    uint32_t* row = g.values + static_cast<size_t>(v) * Qg + lane;
+    uint32_t best[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) best[c] = ((lsel >> c) & 1u) ? row[32 * c] : 0u;
+    gather_edges<W, WK>(g, G, lv, sb, lsel, beg, end, lane, best, pairs, scanned);
+    uint64_t nw[W];
+#pragma unroll
+    for (int i = 0; i < W; ++i) nw[i] = 0;
+    // the warp owns v's row this level: the entries read above are unchanged
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const bool imp = ((lsel >> c) & 1u) && best[c] < row[32 * c];
+      if (imp) row[32 * c] = best[c];
+      nw[c >> 1] |= static_cast<uint64_t>(__ballot_sync(kFull, imp)) << (32 * (c & 1));
+    }
+    bool app = false;
+    if (lane == 0 && mask_any<W>(nw)) {
+#pragma unroll
+      for (int i = 0; i < W; ++i) {
+        if (!nw[i]) continue;
+        atomic_or64(lv.fnext + static_cast<size_t>(v) * W + i, nw[i]);
+        uni[i] |= nw[i];
+        improved += __popcll(nw[i]);
+      }
+      app = atomicMax(g.stamp + v, lv.level + 1) < lv.level + 1;
+    }
+    warp_append(app, v, app ? degree_of<OT>(G.row, v) : 0, lv.nlist, lv.ncount, lv.nedges, lane);
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(improved, &g.ctl->lc.improved, lane);
+  warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);
+  warp_add(scanned, &g.ctl->lc.spull_edges, lane);
+  warp_add(verts, &g.ctl->lc.spull_vertices, lane);
+}
+
+// Gather level, heavy vertices (in-degree > heavy_degree): a CTA takes a
+// chunk of kHeavyChunk in-edges, its warps min-reduce slices into shared
+// memory, and the chunk's result is committed with one atomicMin per slot.
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->sdir != kDirPull || G.n_pheavy == 0) return;
+  const LevelView lv = level_view(g);
+  constexpr int C = 2 * W;
+  __shared__ uint32_t s_best[C * 32];
+  __shared__ int32_t s_h;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const uint64_t* sb = ctl->sssp_bits;
+  const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long improved = 0, pairs = 0;
+  unsigned scanned = 0;
+  for (int64_t ch = blockIdx.x; ch < G.pheavy_chunks; ch += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = G.n_pheavy - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (G.pheavy_chunk_start[mid] <= ch) lo = mid;
+        else hi = mid - 1;
+      }
+      s_h = lo;
+    }
+    for (int i = threadIdx.x; i < C * 32; i += blockDim.x) s_best[i] = 0xffffffffu;
+    __syncthreads();
+    const int h = s_h;
+    const int32_t v = G.pheavy[h];
+    const int64_t beg = row_at<OT>(G.prow, v);
+    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+    const int64_t cb = beg + (ch - G.pheavy_chunk_start[h]) * kHeavyChunk;
+    const int64_t ce = min(end, cb + kHeavyChunk);
+    if (threadIdx.x == 0 && ch == G.pheavy_chunk_start[h]) atomicAdd(&g.ctl->lc.spull_vertices, 1ULL);
+    const int64_t seg = (ce - cb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int64_t wb = cb + wib * seg;
+    const int64_t we = min(ce, wb + seg);
+    uint32_t best[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) best[c] = 0xffffffffu;
+    gather_edges<W, WK>(g, G, lv, sb, lsel, wb, we, lane, best, pairs, scanned);
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+      if (best[c] != 0xffffffffu) atomicMin(&s_best[32 * c + lane], best[c]);
+    __syncthreads();
+    // commit: warp wib takes chunks wib, wib + 8, ...
+    bool any = false;
+    for (int c = wib; c < C; c += kWarpsPerBlock) {
+      const int q = 32 * c + lane;
+      bool imp = false;
+      if ((lsel >> c) & 1u) {
+        const uint32_t b = s_best[q];
+        uint32_t* p = g.values + static_cast<size_t>(v) * Qg + q;
+        if (b < *p) imp = b < atomicMin(p, b);
+      }
+      const unsigned m = __ballot_sync(kFull, imp);
+      if (m) {
+        any = true;
+        if (lane == 0) {
+          const uint64_t bits = static_cast<uint64_t>(m) << (32 * (c & 1));
+          atomic_or64(lv.fnext + static_cast<size_t>(v) * W + (c >> 1), bits);
+          uni[c >> 1] |= bits;
+          improved += __popc(m);
+        }
+      }
+    }
+    bool app = false;
+    if (any && lane == 0) app = atomicMax(g.stamp + v, lv.level + 1) < lv.level + 1;
+    warp_append(app, v, app ? degree_of<OT>(G.row, v) : 0, lv.nlist, lv.ncount, lv.nedges, lane);
+    __syncthreads();
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(improved, &g.ctl->lc.improved, lane);
+  warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);
+  warp_add(scanned, &g.ctl->lc.spull_edges, lane);
+}
+
 // --------------------------------------------------------- level control
 __device__ __forceinline__ int32_t decide_dir(const LevelCtl* ctl, unsigned long long count,
                                               unsigned long long edges, bool has_bfs) {
@@ -1089,6 +1333,17 @@ __device__ __forceinline__ int32_t decide_dir(const LevelCtl* ctl, unsigned long
   if (ctl->mode == 1) return kDirPull;   // CGP_MODE_PULL
   return (edges >= ctl->pull_edge_threshold || count >= ctl->pull_vertex_threshold)
              ? kDirPull : kDirPush;
+}
+
+// SSSP direction of the next level: gather once the frontier's edges reach
+// the threshold (dense levels), scatter otherwise.
+__device__ __forceinline__ int32_t decide_sdir(const LevelCtl* ctl, unsigned long long edges,
+                                               bool has_sssp) {
+  if (!has_sssp || !ctl->sssp_gather) return kDirPush;
+  if (ctl->forced_dir >= 0) return ctl->forced_dir;
+  if (ctl->mode == 0) return kDirPush;
+  if (ctl->mode == 1) return kDirPull;
+  return edges >= ctl->sssp_pull_edge_threshold ? kDirPull : kDirPush;
 }
 
 template <int W>
@@ -1131,6 +1386,10 @@ __global__ void k_level_end(GroupDev g) {
     p.sssp_pairs = ctl->lc.sssp_pairs;
     p.sssp_active = ctl->lc.sssp_active;
     p.improved = ctl->lc.improved;
+    p.spull_vertices = ctl->lc.spull_vertices;
+    p.spull_edges = ctl->lc.spull_edges;
+    p.sdir = ctl->sdir;
+    p.reserved = 0;
     g.prof[l] = p;
   }
   ctl->total.new_pairs += ctl->lc.new_pairs;
@@ -1139,7 +1398,9 @@ __global__ void k_level_end(GroupDev g) {
   ctl->total.sssp_pairs += ctl->lc.sssp_pairs;
   ctl->total.sssp_active += ctl->lc.sssp_active;
   ctl->total.improved += ctl->lc.improved;
-  ctl->lc = LevelCounters{0, 0, 0, 0, 0, 0};
+  ctl->total.spull_vertices += ctl->lc.spull_vertices;
+  ctl->total.spull_edges += ctl->lc.spull_edges;
+  ctl->lc = LevelCounters{};
   ctl->dense_count = 0;
   ctl->total_frontier += ctl->count[par];
   ctl->total_edges += ctl->edges[par];
@@ -1154,6 +1415,7 @@ __global__ void k_level_end(GroupDev g) {
   for (int i = 0; i < W; ++i) ctl->active[par][i] = 0;
   compute_expand<W>(ctl, g.slots, g.Qg, l + 1);
   ctl->dir = decide_dir(ctl, nextc, ctl->edges[par ^ 1], any_bits<W>(ctl->bfs_bits));
+  ctl->sdir = decide_sdir(ctl, ctl->edges[par ^ 1], any_bits<W>(ctl->sssp_bits));
   if (nextc == 0 || (ctl->max_iterations > 0 && l + 1 >= ctl->max_iterations)) {
     ctl->done = 1;
     return;
@@ -1202,6 +1464,7 @@ __global__ void k_seed(GroupDev g, DevGraph G) {
   if (threadIdx.x == 0) {
     compute_expand<W>(ctl, g.slots, g.Qg, 0);
     ctl->dir = decide_dir(ctl, ctl->count[0], ctl->edges[0], any_bits<W>(ctl->bfs_bits));
+    ctl->sdir = decide_sdir(ctl, ctl->edges[0], any_bits<W>(ctl->sssp_bits));
     if (ctl->count[0] == 0) ctl->done = 1;
   }
 }

@@ -101,6 +101,7 @@ __global__ void k_admit(GroupDev g, DevGraph G, const AdmitReq* reqs, int n) {
   if (threadIdx.x == 0 && ctl->count[par] > 0) {
     ctl->done = 0;
     ctl->dir = decide_dir(ctl, ctl->count[par], ctl->edges[par], any_bits<W>(ctl->bfs_bits));
+    ctl->sdir = decide_sdir(ctl, ctl->edges[par], any_bits<W>(ctl->sssp_bits));
   }
 }
 

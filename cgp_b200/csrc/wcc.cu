@@ -92,10 +92,29 @@ __global__ void __launch_bounds__(kBlock) k_uf_hook(const void* row, const int32
   }
 }
 
-__global__ void k_uf_labels(int32_t* parent, uint32_t* labels, int64_t V) {
+// Root of x without shortening the path.  The label pass writes roots into
+// the parent array itself, so it must not also store shortcuts: a late
+// shortcut store to parent[y] could replace y's finished label (its root)
+// with an intermediate ancestor.
+__device__ __forceinline__ int32_t uf_root(const int32_t* parent, int32_t x) {
+  const volatile int32_t* p = parent;
+  int32_t cur = x;
+  for (;;) {
+    const int32_t next = p[cur];
+    if (next == cur) return cur;
+    cur = next;
+  }
+}
+
+// labels[v] = root(v), in place over the parent array: each entry is written
+// once, by its own thread, with an ancestor of v, so concurrent readers still
+// follow valid parent chains.
+__global__ void k_uf_labels(int32_t* parent, int64_t V) {
   for (int64_t v = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
-       v += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    labels[v] = static_cast<uint32_t>(uf_find(parent, static_cast<int32_t>(v)));
+       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t r = uf_root(parent, static_cast<int32_t>(v));
+    reinterpret_cast<volatile int32_t*>(parent)[v] = r;
+  }
 }
 
 __global__ void k_broadcast(const uint32_t* labels, int64_t V, OutMap om, int colidx) {
@@ -118,7 +137,7 @@ void wcc_labels(GraphImpl* g, uint32_t* labels, cudaStream_t s) {
   else
     k_uf_hook<int32_t><<<blocks, kBlock, 0, s>>>(g->row.p, g->col.as<int32_t>(), parent, g->V,
                                                 g->symmetric ? 1 : 0);
-  k_uf_labels<<<blocks, kBlock, 0, s>>>(parent, labels, g->V);
+  k_uf_labels<<<blocks, kBlock, 0, s>>>(parent, g->V);
   ck(cudaGetLastError(), "wcc");
 }
 

@@ -106,7 +106,9 @@ typedef struct {
   int32_t discard_results;    /* run_options::discard_results                    */
   int32_t profile_kernels;    /* time kernel classes with CUDA events (slower; no graphs) */
   int32_t dense_unroll;       /* edges per step of the dense SSSP kernel: 1 or 2; 0 = 1 */
-  int32_t reserved[4];
+  double sssp_pull_edge_ratio; /* SSSP levels gather (pull) when frontier edges >= ratio * E;
+                                  <= 0: always scatter (push)                              */
+  int32_t reserved[2];
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 
@@ -124,6 +126,10 @@ typedef struct {
   uint64_t sssp_pairs;       /* (edge, active query) relaxations attempted           */
   uint64_t sssp_active;      /* active SSSP bits summed over frontier vertices       */
   uint64_t improved;         /* SSSP (query, vertex) improvements                    */
+  uint64_t sssp_pull_vertices; /* vertices an SSSP gather level scanned                 */
+  uint64_t sssp_pull_edges;  /* in-edges an SSSP gather level scanned                    */
+  int32_t sssp_mode;         /* SSSP direction of the level: 0 push (scatter), 1 pull (gather) */
+  int32_t reserved;
 } cgp_level_profile;
 
 /* run_result_t scalars (result.hxx:49-66). */
@@ -146,13 +152,15 @@ typedef struct {
   uint64_t sssp_pairs;
   uint64_t sssp_active;
   uint64_t improved;
+  uint64_t sssp_pull_vertices;
+  uint64_t sssp_pull_edges;
 } cgp_stats;
 
 /* Per-kernel-class CUDA-event times of the last cgp_batch_run on this thread
  * that had profile_kernels set. */
 typedef struct {
   double ms[12];       /* clear, bfs_push, bfs_pull, sssp_push, level_end, init, output, wcc,
-                          sssp_dense, sssp_heavy */
+                          sssp_dense, sssp_heavy, sssp_pull */
   int64_t launches[12];
 } cgp_kernel_profile;
 

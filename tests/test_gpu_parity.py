@@ -156,6 +156,15 @@ def test_wcc_parity(rmat_u32, grid_f32):
         np.testing.assert_array_equal(r.values[:, 0], oracle.wcc_label_propagation(g))
 
 
+def test_wcc_labels_stable_over_repeated_runs(rmat_u32, grid_f32):
+    # the label pass runs concurrently with nothing that may rewrite a
+    # finished label; repeated runs catch a late path-shortening store
+    for g, graph in (rmat_u32, grid_f32):
+        want = oracle.wcc_components(g)
+        for _ in range(40):
+            np.testing.assert_array_equal(cgp.run("wcc", graph, [0]).values[:, 0], want)
+
+
 def test_khop_parity(rmat_u32):
     g, graph = rmat_u32
     src = g.pick_sources(60, seed=14)
@@ -365,3 +374,96 @@ def test_sssp_execution_knobs_do_not_change_results(rmat_u32, opts):
     r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
                       cgp.RunOptions(**opts), layout="query")
     np.testing.assert_array_equal(r.values, ref)
+
+
+# ------------------------------------------------------------- SSSP gather
+# Dense SSSP levels gather over in-edges (pull CSR + reverse-edge weights).
+@pytest.mark.parametrize("opts", [
+    dict(traversal_mode="pull"),
+    dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.02),
+    dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.0),
+    dict(traversal_mode="pull", heavy_degree=16),
+    dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.05, heavy_degree=32, mask_words=16),
+])
+def test_sssp_gather_parity(rmat_u32, rmat_f32, grid_f32, opts):
+    for g, graph in (rmat_u32, rmat_f32, grid_f32):
+        src = g.pick_sources(70, seed=31)
+        ref, _ = oracle.batch("sssp", g, src)
+        r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                          cgp.RunOptions(profile_iterations=True, **opts), layout="query")
+        np.testing.assert_array_equal(r.values, ref)
+        modes = {p.sssp_mode for p in r.iteration_profiles}
+        if opts.get("sssp_pull_edge_ratio", 1) == 0.0:
+            assert modes == {"push"}
+        else:
+            assert "pull" in modes
+
+
+def _weighted_variant(g, w, kind):
+    return cgp.HostCsr(g.row_offsets, g.col_indices,
+                       np.ascontiguousarray(w, np.uint32 if kind == "u32" else np.float32))
+
+
+@pytest.mark.parametrize("kind", ["u32", "f32"])
+def test_sssp_gather_uses_reverse_edge_weights(kind):
+    """Symmetric structure, asymmetric weights: a gather must relax u -> v
+    with w(u, v), the weight stored in u's list, not v's."""
+    rng = np.random.default_rng(41)
+    base = cgp.gen_rmat(11, 8, seed=42)
+    w = (rng.integers(1, 100, base.num_edges) if kind == "u32"
+         else rng.uniform(0.5, 50.0, base.num_edges))
+    g = _weighted_variant(base, w, kind)
+    graph = cgp.CsrGraph(g)
+    assert graph.symmetric
+    src = g.pick_sources(40, seed=43)
+    ref, _ = oracle.batch("sssp", g, src)
+    for mode in ("push", "pull", "hybrid"):
+        r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                          cgp.RunOptions(traversal_mode=mode, sssp_pull_edge_ratio=0.01),
+                          layout="query")
+        np.testing.assert_array_equal(r.values, ref)
+
+
+def test_sssp_gather_unsorted_lists_and_directed():
+    """Unsorted adjacency lists (the transpose is stored) and a directed
+    weighted graph (gather over the transposed CSR and weights)."""
+    rng = np.random.default_rng(44)
+    base = cgp.gen_rmat(11, 8, seed=45)
+    row, col = base.row_offsets, base.col_indices.copy()
+    for v in range(base.num_vertices):  # shuffle every list in place
+        a, b = row[v], row[v + 1]
+        col[a:b] = rng.permutation(col[a:b])
+    w = rng.integers(1, 64, base.num_edges)
+    g1 = cgp.HostCsr(row, col, np.ascontiguousarray(w, np.uint32))
+    V = 2500
+    s = rng.integers(0, V, 30000)
+    d = rng.integers(0, V, 30000)
+    dg = cgp.csr_from_edges(V, s, d, symmetrize=False)
+    g2 = cgp.HostCsr(dg.row_offsets, dg.col_indices,
+                     np.ascontiguousarray(rng.uniform(1.0, 10.0, dg.num_edges), np.float32))
+    for g in (g1, g2):
+        graph = cgp.CsrGraph(g)
+        src = g.pick_sources(50, seed=46)
+        ref, _ = oracle.batch("sssp", g, src)
+        for mode in ("pull", "hybrid"):
+            r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                              cgp.RunOptions(traversal_mode=mode, sssp_pull_edge_ratio=0.01,
+                                             heavy_degree=24), layout="query")
+            np.testing.assert_array_equal(r.values, ref)
+
+
+@pytest.mark.parametrize("ratio", [0.01, 0.5])
+def test_mixed_batch_with_sssp_gather(rmat_u32, ratio):
+    g, graph = rmat_u32
+    src = g.pick_sources(150, seed=47)
+    kinds = ["bfs", "sssp", "khop", "sssp"]
+    descs = [cgp.QueryDescriptor(int(s), kinds[i % 4], 2) for i, s in enumerate(src)]
+    r = cgp.run_heterogeneous(graph, cgp.HybridQueryBatch(descs),
+                              options=cgp.RunOptions(sssp_pull_edge_ratio=ratio), layout="query")
+    for i, d in enumerate(descs):
+        if d.kind == "bfs":
+            np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source))
+        elif d.kind == "khop":
+            np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source, 2))
+        else:
+            np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
