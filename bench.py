@@ -53,6 +53,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-one-query", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-layout", default="vertex", choices=["vertex", "query"])
     p.add_argument("--mode", default="hybrid")
     p.add_argument("--pull-edge-ratio", type=float, default=0.20)
     p.add_argument("--pull-frontier-ratio", type=float, default=0.15)
@@ -156,31 +157,60 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- roofline
-def level_bytes(profiles, kind, V, W, ob=4, qs=0):
-    """Algorithmic bytes per kernel class from the per-level counters.
+def level_bytes(p, kind, V, W, ob=4, qs=0):
+    """Algorithmic bytes of one level from its device counters.
     BFS push: U(2o+Wb+4) + D(4+2Wb) + 4N + Wb U'
     BFS pull: 2 V Wb + P 2o + S(4+Wb) + 4N
     SSSP push (scatter): U(2o+Wb+4) + D(4+4+Wb) + 4 sum(popc) + 8 A + Wb U'
     SSSP pull (gather):  2o V + 4 Qs P + S(4+4+Wb) + 4 A + 4 I + Wb U'
     (A = (edge, active query) pairs, I = improved entries, Qs = SSSP slots)"""
     Wb = 8 * W
-    out = {"bfs_push": 0, "bfs_pull": 0, "sssp_relax": 0}
+    U, D, N, Un = p.frontier_size, p.frontier_edges, p.new_pairs, p.next_size
+    if kind == "bfs":
+        if p.mode == "push":
+            return "bfs_push", U * (2 * ob + Wb + 4) + D * (4 + 2 * Wb) + 4 * N + Wb * Un
+        return "bfs_pull", 2 * V * Wb + p.pull_vertices * 2 * ob + p.pull_edges * (4 + Wb) + 4 * N
+    if p.sssp_mode == "push":
+        return "sssp_scatter", (U * (2 * ob + Wb + 4) + D * (4 + 4 + Wb) + 4 * p.sssp_active
+                                + 8 * p.sssp_pairs + Wb * Un)
+    return "sssp_gather", (2 * ob * V + 4 * qs * p.sssp_pull_vertices
+                           + p.sssp_pull_edges * (4 + 4 + Wb) + 4 * p.sssp_pairs
+                           + 4 * p.improved + Wb * Un)
+
+
+# kernels that do the work of each level class
+CLASS_KERNELS = {
+    "bfs_push": "k_bfs_push, k_bfs_push_heavy",
+    "bfs_pull": "k_bfs_pull, k_bfs_pull_heavy(_commit)",
+    "sssp_scatter": "k_sssp_push, k_sssp_dense, k_sssp_push_heavy",
+    "sssp_gather": "k_sssp_pull_vec, k_sssp_pull_heavy_vec",
+}
+
+
+def level_classes(profiles, kind, V, W, qs=0):
+    """Per level class: levels, kernel ms (CUDA events on the launching
+    stream, every kernel of the level) and algorithmic bytes."""
+    out = {}
     for p in profiles:
-        U, D, N, Un = p.frontier_size, p.frontier_edges, p.new_pairs, p.next_size
-        if kind == "bfs":
-            if p.mode == "push":
-                out["bfs_push"] += U * (2 * ob + Wb + 4) + D * (4 + 2 * Wb) + 4 * N + Wb * Un
-            else:
-                out["bfs_pull"] += (2 * V * Wb + p.pull_vertices * 2 * ob
-                                    + p.pull_edges * (4 + Wb) + 4 * N)
-        elif p.sssp_mode == "push":
-            out["sssp_relax"] += (U * (2 * ob + Wb + 4) + D * (4 + 4 + Wb) + 4 * p.sssp_active
-                                  + 8 * p.sssp_pairs + Wb * Un)
-        else:
-            out["sssp_relax"] += (2 * ob * V + 4 * qs * p.sssp_pull_vertices
-                                  + p.sssp_pull_edges * (4 + 4 + Wb) + 4 * p.sssp_pairs
-                                  + 4 * p.improved + Wb * Un)
+        name, b = level_bytes(p, kind, V, W, qs=qs)
+        c = out.setdefault(name, {"ms": 0.0, "launches": 0, "bytes": 0})
+        c["ms"] += p.kernel_ms
+        c["launches"] += 1
+        c["bytes"] += b
     return out
+
+
+def ncu_traffic(workload, cls):
+    """DRAM bytes per level of a class, from a committed ncu summary
+    (profiles/dram_traffic.txt lines: workload class bytes_per_level)."""
+    f = ROOT / "profiles" / "dram_traffic.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 3 and not line.startswith("#") and parts[0] == workload and parts[1] == cls:
+            return float(parts[2])
+    return None
 
 
 def measured_peaks():
@@ -215,6 +245,16 @@ def cpu_reference_sample(g, bfs_src, sssp_src, threads):
     return dt, edges, kind, (b, s)
 
 
+def workload_config(args, g, comp_v, world):
+    """The workload keys shared by both arms' JSON lines."""
+    return {"workload": workload_name(args), "graph": "rmat", "scale": args.scale,
+            "edge_factor": args.edge_factor, "a_b_c": [0.57, 0.19, 0.19],
+            "V": g.num_vertices, "E": g.num_edges, "weights": "u32 uniform [1,64]",
+            "queries_per_gpu": {"bfs": args.nbfs, "sssp": args.nsssp},
+            "largest_component_vertices": comp_v,
+            "parallelism": f"query-sharded x{world}"}
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -245,8 +285,7 @@ def run_reference_arm(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * t / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": workload_name(args), "scale": args.scale,
-                   "edge_factor": args.edge_factor, "V": g.num_vertices, "E": g.num_edges},
+        "config": workload_config(args, g, comp_v, args.gpus),
         "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -448,28 +487,17 @@ def main():
                                                            profile_iterations=True), out=out_s)
           if sssp_d else empty)
     W = pb.mask_words or ps.mask_words
-    bytes_b = level_bytes(pb.iteration_profiles, "bfs", V, W)
-    bytes_s = level_bytes(ps.iteration_profiles, "sssp", V, ps.mask_words, qs=len(sssp_d))
-    kclass = {}
-    for name in ("bfs_push", "bfs_pull"):
-        if name in pb.kernel_profile:
-            ms_k, n_k = pb.kernel_profile[name]
-            kclass[name] = {"ms": ms_k, "launches": n_k, "bytes": bytes_b[name]}
-    if "sssp_push" in ps.kernel_profile:
-        # one SSSP level = scatter (tile + dense + heavy) or gather (light +
-        # heavy) kernels; bytes are counted per level
-        ms_k = sum(ps.kernel_profile.get(k, (0.0, 0))[0]
-                   for k in ("sssp_push", "sssp_dense", "sssp_heavy", "sssp_pull"))
-        n_k = ps.kernel_profile["sssp_push"][1]
-        kclass["sssp_relax"] = {"ms": ms_k, "launches": n_k, "bytes": bytes_s["sssp_relax"]}
+    kclass = {**level_classes(pb.iteration_profiles, "bfs", V, W),
+              **level_classes(ps.iteration_profiles, "sssp", V, ps.mask_words, qs=len(sssp_d))}
     level_trace = {
-        "bfs": [[p.mode, p.frontier_size, p.frontier_edges, p.new_pairs, p.pull_edges]
-                for p in pb.iteration_profiles],
+        "bfs": [[p.mode, p.frontier_size, p.frontier_edges, p.new_pairs, p.pull_edges,
+                 round(p.kernel_ms, 3)] for p in pb.iteration_profiles],
         "sssp": [[p.sssp_mode, p.frontier_size, p.frontier_edges, p.sssp_active, p.sssp_pairs,
-                  p.improved, p.sssp_pull_edges] for p in ps.iteration_profiles],
-        "columns": {"bfs": ["mode", "frontier", "frontier_edges", "new_pairs", "pull_edges"],
+                  p.improved, p.sssp_pull_edges, round(p.kernel_ms, 3)]
+                 for p in ps.iteration_profiles],
+        "columns": {"bfs": ["mode", "frontier", "frontier_edges", "new_pairs", "pull_edges", "ms"],
                     "sssp": ["mode", "frontier", "frontier_edges", "active_bits", "pairs",
-                             "improved", "pull_edges"]},
+                             "improved", "pull_edges", "ms"]},
         "kernel_ms": {"bfs": pb.kernel_profile, "sssp": ps.kernel_profile},
     }
     peak, peak_src = measured_peaks()
@@ -478,9 +506,11 @@ def main():
     if dom:
         k = kclass[dom]
         achieved = k["bytes"] / (k["ms"] / 1e3) / 1e9
-        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+        roofline = {"bound": "hbm", "kernel": f"{dom} levels ({CLASS_KERNELS[dom]})",
+                    "achieved": achieved, "peak": peak,
                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-                    "traffic": None, "bytes_per_launch": k["bytes"] / max(1, k["launches"]),
+                    "traffic": ncu_traffic(workload_name(args), dom),
+                    "per": "level", "bytes_per_launch": k["bytes"] / max(1, k["launches"]),
                     "ms_per_launch": k["ms"] / max(1, k["launches"]),
                     "classes": {n: {"ms": v["ms"], "launches": v["launches"],
                                     "GBps": v["bytes"] / max(v["ms"], 1e-9) / 1e6}
@@ -515,19 +545,25 @@ def main():
                      "sssp_ms_per_query": ts1,
                      "sample": f"{nb1} BFS + {ns1} SSSP single-query runs, scaled to the batch"}
 
-    # ---- e2e: the public API with host buffers (pinned), copies inside
+    # ---- e2e: the public API with host buffers (pinned), copies inside.
+    # One heterogeneous call per step (run_heterogeneous, the reference's
+    # hybrid-batch entry point): the library runs the BFS and the SSSP
+    # queries as separate groups and copies each group's result block to the
+    # host while the next group traverses.
     e2e = None
-    if args.e2e_steps > 0:
-        hb = torch.empty((V, len(bfs_d)), dtype=torch.int32, pin_memory=True)
-        hs = torch.empty((V, len(sssp_d)), dtype=torch.int32, pin_memory=True)
-        eopts_b = dataclasses.replace(opts_b, stream=0)
-        eopts_s = dataclasses.replace(opts_s, stream=0)
+    if args.e2e_steps > 0 and (bfs_d or sssp_d):
+        qmaj = args.e2e_layout == "query"
+        nq = len(bfs_d) + len(sssp_d)
+        host = torch.empty((nq, V) if qmaj else (V, nq), dtype=torch.int32, pin_memory=True)
+        eopts = dataclasses.replace(opts_s if sssp_d else opts_b, stream=0,
+                                    pull_edge_ratio=opts_b.pull_edge_ratio,
+                                    pull_frontier_ratio=opts_b.pull_frontier_ratio)
+        batch = cgp.HybridQueryBatch(bfs_d + sssp_d)
+
         def e2e_step():
-            if bfs_d:
-                cgp.run_batch(graph, bfs_d, eopts_b, out=hb)
-            if sssp_d:
-                cgp.run_batch(graph, sssp_d, eopts_s, out=hs)
-        e2e_step()
+            return cgp.run_heterogeneous(graph, batch, options=eopts, out=host,
+                                         layout="query" if qmaj else "vertex")
+        r_e2e = e2e_step()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
@@ -535,11 +571,21 @@ def main():
         t_e2e = time.perf_counter() - t0
         t_e2e = allreduce(t_e2e, dist.ReduceOp.MAX if world > 1 else None)
         e_edges = allreduce(edges_step * args.e2e_steps, dist.ReduceOp.SUM if world > 1 else None)
+        # spot check: the host copy equals the device-resident results
+        hv = host.numpy()
+        col = (lambda j: hv[j]) if qmaj else (lambda j: hv[:, j])
+        same = True
+        for j in ((0, len(bfs_d) - 1) if bfs_d else ()):
+            same &= bool(np.array_equal(col(j), out_b[:, j].cpu().numpy()))
+        for j in ((0, len(sssp_d) - 1) if sssp_d else ()):
+            same &= bool(np.array_equal(col(len(bfs_d) + j), out_s[:, j].cpu().numpy()))
         e2e = {"value": e_edges / t_e2e / 1e9, "unit": "GTEPS",
-               "h2d_bytes_per_step": 16 * (len(bfs_d) + len(sssp_d)),
-               "d2h_bytes_per_step": 4 * V * (len(bfs_d) + len(sssp_d)),
+               "h2d_bytes_per_step": 16 * nq,
+               "d2h_bytes_per_step": 4 * V * nq,
                "steps": args.e2e_steps, "ms_per_step": 1e3 * t_e2e / args.e2e_steps,
-               "output": "pinned host buffers, vertex-major int32/uint32"}
+               "groups": r_e2e.groups, "matches_device": same,
+               "output": f"one pinned host buffer, {'query' if qmaj else 'vertex'}-major "
+                         f"int32/uint32 [{'Q][V' if qmaj else 'V][Q'}]"}
 
     # ---- serving: continuous batching on the same graph, Poisson arrivals
     serving = None
@@ -579,11 +625,8 @@ def main():
             "steps": args.steps, "warmup": max(3, args.warmup),
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": workload_name(args), "graph": "rmat", "scale": args.scale,
-                       "edge_factor": args.edge_factor, "a_b_c": [0.57, 0.19, 0.19],
-                       "V": V, "E": g.num_edges, "weights": "u32 uniform [1,64]",
-                       "queries_per_gpu": {"bfs": len(bfs_d), "sssp": len(sssp_d)},
-                       "mask_words": W, "largest_component_vertices": comp_v,
+            "config": {**workload_config(args, g, comp_v, world),
+                       "mask_words": W,
                        "traversal_mode": args.mode,
                        "tuned": None if args.no_autotune else {
                            "bfs": {"mask_words": opts_b.mask_words, "heavy_degree": opts_b.heavy_degree,
@@ -594,8 +637,7 @@ def main():
                            "tuning_s": tune_s},
                        "l2": f"inputs larger than L2: CSR {4 * (V + 1 + 2 * g.num_edges) / 2**20:.0f} MiB "
                              f"+ outputs {8 * V * (len(bfs_d) + len(sssp_d)) / 2**30:.1f} GiB "
-                             f"per step, re-initialised every step (no flush)",
-                       "parallelism": f"query-sharded x{world}"},
+                             f"per step, re-initialised every step (no flush)"},
             "queries_per_s": qps,
             "bfs": {"ms": t_b / args.steps,
                     "gteps": comp_edges * len(bfs_d) / max(t_b / args.steps / 1e3, 1e-12) / 1e9,

@@ -50,7 +50,7 @@ class CgpLevelProfile(Structure):
                 ("pull_vertices", c_uint64), ("pull_edges", c_uint64), ("sssp_pairs", c_uint64),
                 ("sssp_active", c_uint64), ("improved", c_uint64),
                 ("sssp_pull_vertices", c_uint64), ("sssp_pull_edges", c_uint64),
-                ("sssp_mode", c_int32), ("reserved", c_int32)]
+                ("sssp_mode", c_int32), ("kernel_ms", c_float)]
 
 
 class CgpStats(Structure):

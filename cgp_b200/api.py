@@ -329,6 +329,7 @@ class IterationProfile:
     sssp_pull_vertices: int = 0
     sssp_pull_edges: int = 0
     sssp_mode: str = "push"
+    kernel_ms: float = 0.0
 
 
 @dataclass
@@ -408,7 +409,8 @@ def run_batch(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpt
                                      p.frontier_edges, p.next_size, p.query_convergence_mask,
                                      p.new_pairs, p.pull_vertices, p.pull_edges, p.sssp_pairs,
                                      p.sssp_active, p.improved, p.sssp_pull_vertices,
-                                     p.sssp_pull_edges, "pull" if p.sssp_mode else "push")
+                                     p.sssp_pull_edges, "pull" if p.sssp_mode else "push",
+                                     p.kernel_ms)
                     for p in buf[:cnt.value]]
     kprof = {}
     if options.profile_kernels:

@@ -49,6 +49,8 @@ Workspace::Workspace(int dev) : device(dev) {
      "cudaHostAlloc(slots)");
   ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
   ck(cudaStreamCreateWithFlags(&capture, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cudaEventCreateWithFlags(&out_ready, cudaEventDisableTiming), "cudaEventCreate");
   for (auto& e : ev) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
   ctl.ensure(sizeof(LevelCtl));
   slots.ensure(kMaxWords * 64 * sizeof(SlotDev));
@@ -65,6 +67,8 @@ Workspace::~Workspace() {
   if (hslots) cudaFreeHost(hslots);
   if (stream) cudaStreamDestroy(stream);
   if (capture) cudaStreamDestroy(capture);
+  if (copy) cudaStreamDestroy(copy);
+  if (out_ready) cudaEventDestroy(out_ready);
   for (auto& e : ev)
     if (e) cudaEventDestroy(e);
 }
@@ -263,6 +267,8 @@ struct Grids {
   int dense2;
   int gather;
   int gather_heavy;
+  int gather_vec;
+  int gather_heavy_vec;
 };
 
 struct LevelLaunch {
@@ -273,6 +279,7 @@ struct LevelLaunch {
   bool has_sssp;
   bool pull;
   bool spull;        // SSSP gather kernels are part of the level
+  bool gvec;         // rows allow the vectorised gather (alignment, width)
   int dense_unroll;  // edges per step of the dense SSSP kernel (1 or 2)
   KernelTimer* kt;   // per-class event timing (non-graph runs only)
 };
@@ -331,10 +338,16 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
     }
     if (L.spull) {
       if (kt) kt->mark(kClassSsspPull, s);
-      k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
+      if (L.gvec)
+        k_sssp_pull_vec<W, OT, WK><<<L.gr.gather_vec, kBlock, 0, s>>>(L.g, L.G);
+      else
+        k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
       ++n;
       if (L.G.n_pheavy) {
-        k_sssp_pull_heavy<W, OT, WK><<<L.gr.gather_heavy, kBlock, 0, s>>>(L.g, L.G);
+        if (L.gvec)
+          k_sssp_pull_heavy_vec<W, OT, WK><<<L.gr.gather_heavy_vec, kBlock, 0, s>>>(L.g, L.G);
+        else
+          k_sssp_pull_heavy<W, OT, WK><<<L.gr.gather_heavy, kBlock, 0, s>>>(L.g, L.G);
         ++n;
       }
     }
@@ -349,7 +362,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
 template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
   static int tile = 0, heavy = 0, dense = 0, dense2 = 0, gather = 0, gather_heavy = 0;
+  static int gather_vec = 0, gather_heavy_vec = 0;
   if (tile == 0) {
+    gather_vec = occupancy_grid(k_sssp_pull_vec<W, OT, WK>, sms);
+    gather_heavy_vec = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK>, sms);
     gather = occupancy_grid(k_sssp_pull<W, OT, WK>, sms);
     gather_heavy = occupancy_grid(k_sssp_pull_heavy<W, OT, WK>, sms);
     dense = occupancy_grid(k_sssp_dense<W, OT, WK, 1>, sms);
@@ -369,6 +385,8 @@ Grids grids_t(int sms) {
   g.dense2 = dense2;
   g.gather = gather;
   g.gather_heavy = gather_heavy;
+  g.gather_vec = gather_vec;
+  g.gather_heavy_vec = gather_heavy_vec;
   return g;
 }
 
@@ -546,6 +564,12 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   if (!g->can_gather()) mode = CGP_MODE_PUSH;
   L.pull = mode != CGP_MODE_PUSH;
   L.spull = spec.has_sssp && sssp_gather_on(g, o);
+  {
+    // vector gather: kElem-slot vectors must stay inside rows and be aligned
+    const int elem = spec.W == 1 ? 2 : 4;
+    L.gvec = L.g.values != nullptr && spec.Qg % elem == 0 &&
+             reinterpret_cast<uintptr_t>(L.g.values) % (4 * elem) == 0;
+  }
   L.dense_unroll = o.dense_unroll == 2 ? 2 : 1;
   L.kt = kt;
   if (!o.use_cuda_graph || kt != nullptr) {
@@ -592,6 +616,9 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
     int n = per_chunk;
     if (max_levels > 0) n = std::min(n, max_levels - enqueued);
     if (n <= 0) break;
+    double before = 0;
+    if (kt)
+      for (int c = 0; c < kNumClasses; ++c) before += kt->ms[c];
     spec.launches += enqueue_levels(g, ws, spec, o, s, n, kt);
     enqueued += n;
     ck(cudaMemcpyAsync(&snap[chunk & 1], ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost, s),
@@ -601,6 +628,9 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
     if (kt) {
       kt->flush();
       ck(cudaEventSynchronize(ws->ev[chunk & 1]), "sync level");
+      double after = 0;
+      for (int c = 0; c < kNumClasses; ++c) after += kt->ms[c];
+      out->level_ms.push_back(static_cast<float>(after - before));
       stop = snap[chunk & 1].done != 0;
     } else if (chunk > 0) {
       ck(cudaEventSynchronize(ws->ev[(chunk - 1) & 1]), "sync chunk");
@@ -699,6 +729,7 @@ bool csr_is_symmetric(const std::vector<int64_t>& row, const int32_t* col, int64
 }
 
 thread_local std::vector<LevelProfile> t_profiles;
+thread_local std::vector<float> t_level_ms;  // per-level kernel time (profile_kernels)
 thread_local cgp_kernel_profile t_kernel_profile;
 
 }  // namespace
@@ -881,7 +912,7 @@ cgp_status cgp_last_profiles(cgp_level_profile* out, int32_t cap, int32_t* count
       out[i].sssp_pull_vertices = t_profiles[i].spull_vertices;
       out[i].sssp_pull_edges = t_profiles[i].spull_edges;
       out[i].sssp_mode = t_profiles[i].sdir;
-      out[i].reserved = 0;
+      out[i].kernel_ms = i < static_cast<int>(t_level_ms.size()) ? t_level_ms[i] : 0.0f;
     }
   }
   return CGP_OK;
@@ -952,6 +983,7 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
     int groups = 0;
     int W0 = 0, depth0 = 0;
     t_profiles.clear();
+    t_level_ms.clear();
     if (!wcc_idx.empty()) {
       if (kt) kt->mark(kClassWcc, s);
       ws->wcc.ensure(static_cast<size_t>(V) * 4);
@@ -960,15 +992,47 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
       launches += 3 + wcc_idx.size();
       if (kt) kt->mark(-1, s);
     }
-    // traversal groups of up to 64*W queries, in submission order
-    const int Wmax = choose_words(static_cast<int>(trav_idx.size()), o.mask_words);
-    const int per_group = 64 * Wmax;
-    const bool single = trav_idx.size() <= static_cast<size_t>(per_group);
-    for (size_t b = 0; b < trav_idx.size(); b += per_group) {
-      const int n = static_cast<int>(std::min<size_t>(per_group, trav_idx.size() - b));
+    // Traversal groups of up to 64*W queries, in submission order.  A batch
+    // with many BFS-like and many SSSP queries is split by kind first (each
+    // kind then gets its own groups): the kinds share no state, a pure BFS
+    // group keeps its depths in bit-planes, and a pure SSSP group reads no
+    // BFS slots in its gathers.  Small mixed batches share one group, as in
+    // the reference's hybrid batch.
+    std::vector<std::vector<int>> classes;
+    {
+      std::vector<int> bfs_like, sssp_q;
+      for (int i : trav_idx) (queries[i].kind == CGP_KIND_SSSP ? sssp_q : bfs_like).push_back(i);
+      if (bfs_like.size() >= 64 && sssp_q.size() >= 64) classes = {bfs_like, sssp_q};
+      else if (!trav_idx.empty()) classes = {trav_idx};
+    }
+    struct GroupPlan {
+      const std::vector<int>* cls;
+      size_t begin;
+      int n;
+      int W;
+    };
+    std::vector<GroupPlan> plan;
+    for (const auto& cls : classes) {
+      const int Wc = choose_words(static_cast<int>(cls.size()), o.mask_words);
+      const int per_group = 64 * Wc;
+      for (size_t b = 0; b < cls.size(); b += per_group) {
+        const int n = static_cast<int>(std::min<size_t>(per_group, cls.size() - b));
+        plan.push_back(GroupPlan{&cls, b, n, choose_words(n, o.mask_words)});
+      }
+    }
+    const bool single = plan.size() == 1;
+    // Host output: each group's result block is copied to the host on the
+    // copy stream as soon as it is written, overlapping the next group's
+    // traversal, when its destination is one contiguous block (query-major
+    // rows, or a run of vertex-major columns as a 2D copy).
+    const bool host_out = !out_on_device && !o.discard_results;
+    bool copied_all = host_out;
+    std::vector<char> col_copied(host_out ? nq : 0, 0);
+    for (const GroupPlan& gp : plan) {
+      const int n = gp.n;
       std::vector<cgp_query> gq(n);
-      for (int i = 0; i < n; ++i) gq[i] = queries[trav_idx[b + i]];
-      GroupSpec spec = make_group(gq.data(), n, choose_words(n, o.mask_words), o.depth_mode);
+      for (int i = 0; i < n; ++i) gq[i] = queries[(*gp.cls)[gp.begin + i]];
+      GroupSpec spec = make_group(gq.data(), n, gp.W, o.depth_mode);
       // A device vertex-major output holding exactly this group's columns is
       // used directly as the working value matrix (no copy at the end).
       const bool in_place = out_on_device && !qmajor && single && wcc_idx.empty() &&
@@ -982,7 +1046,7 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
       if (!in_place) {
         if (kt) kt->mark(kClassOutput, s);
         std::vector<int32_t> qmap(n);
-        for (int i = 0; i < n; ++i) qmap[i] = trav_idx[b + i];
+        for (int i = 0; i < n; ++i) qmap[i] = (*gp.cls)[gp.begin + i];
         ws->qmap.ensure(static_cast<size_t>(n) * 4);
         ck(cudaMemcpyAsync(ws->qmap.p, qmap.data(), static_cast<size_t>(n) * 4,
                            cudaMemcpyHostToDevice, s), "upload query map");
@@ -992,6 +1056,23 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
         for (int i = 1; i < n; ++i) m.qmap_contiguous &= qmap[i] == qmap[0] + i ? 1 : 0;
         group_write_output(g, ws.get(), spec, m, qmajor, s);
         if (kt) kt->mark(-1, s);
+        if (host_out && m.qmap_contiguous && wcc_idx.empty()) {
+          ck(cudaEventRecord(ws->out_ready, s), "event");
+          ck(cudaStreamWaitEvent(ws->copy, ws->out_ready, 0), "wait");
+          const size_t q0 = static_cast<size_t>(qmap[0]);
+          char* hbase = static_cast<char*>(out);
+          const char* dbase = reinterpret_cast<const char*>(dout);
+          if (qmajor) {
+            const size_t off = q0 * static_cast<size_t>(V) * 4;
+            ck(cudaMemcpyAsync(hbase + off, dbase + off, static_cast<size_t>(n) * V * 4,
+                               cudaMemcpyDeviceToHost, ws->copy), "copy out");
+          } else {
+            ck(cudaMemcpy2DAsync(hbase + q0 * 4, static_cast<size_t>(nq) * 4, dbase + q0 * 4,
+                                 static_cast<size_t>(nq) * 4, static_cast<size_t>(n) * 4, V,
+                                 cudaMemcpyDeviceToHost, ws->copy), "copy out");
+          }
+          for (int i = 0; i < n; ++i) col_copied[qmap[i]] = 1;
+        }
       }
       launches += spec.launches;
       total.iterations = std::max(total.iterations, r.iterations);
@@ -1011,14 +1092,17 @@ cgp_status cgp_batch_run(cgp_graph* graph, const cgp_query* queries, int32_t nq,
         W0 = spec.W;
         depth0 = spec.depth_mode;
         t_profiles = r.profiles;
+        t_level_ms = r.level_ms;
       }
       ++groups;
     }
     ck(cudaEventRecord(t1, s), "event");
-    if (!out_on_device && !o.discard_results)
+    for (char c : col_copied) copied_all = copied_all && c;
+    if (host_out && !copied_all)
       ck(cudaMemcpyAsync(out, dout, static_cast<size_t>(V) * nq * 4, cudaMemcpyDeviceToHost, s),
          "copy out");
     ck(cudaStreamSynchronize(s), "batch");
+    if (host_out) ck(cudaStreamSynchronize(ws->copy), "copy out");
     float ms = 0;
     cudaEventElapsedTime(&ms, t0, t1);
     cudaEventDestroy(t0);

@@ -109,6 +109,8 @@ struct Workspace {
   dev::SlotDev* hslots = nullptr;  // pinned, kMaxWords*64 entries
   cudaStream_t stream = nullptr;
   cudaStream_t capture = nullptr;
+  cudaStream_t copy = nullptr;     // device->host result copies overlapping later groups
+  cudaEvent_t out_ready = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   uint64_t generation = 1;
   std::map<std::tuple<int, int, int, int, int, int, int, int, uint64_t, uint64_t>, CachedGraph>
@@ -172,6 +174,7 @@ struct GroupRun {
   uint32_t status = 0;
   dev::LevelCounters counters{};
   std::vector<dev::LevelProfile> profiles;
+  std::vector<float> level_ms;  // kernel time per level when kernel classes are timed
 };
 
 // Engine entry points (engine.cu).

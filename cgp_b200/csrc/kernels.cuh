@@ -1324,6 +1324,360 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy(GroupDev g, DevGraph
   warp_add(scanned, &g.ctl->lc.spull_edges, lane);
 }
 
+
+// ------------------------------------------------- SSSP gather, vectorised
+// The same gather with vector loads, for groups whose rows are 16-byte
+// aligned and hold a multiple of the vector width (the usual case): lane l
+// owns the kElem consecutive slots (32r + l)*kElem .. +kElem of each part r,
+// so a row costs kParts vector loads per lane instead of 2W scalar ones.
+// The live in-edges of a 32-edge batch are compacted into shared memory by
+// a ballot prefix, and full groups of kSteps edges are gathered without any
+// per-load predicate.
+template <int W>
+struct GatherVec {
+  static constexpr int kElem = W == 1 ? 2 : 4;      // slots per vector load
+  static constexpr int kParts = 2 * W / kElem;      // vector loads per lane per row
+  static constexpr int kSlots = kParts * kElem;     // slots per lane
+  static constexpr int kSteps = W <= 2 ? 8 : (W == 4 ? 4 : (W == 8 ? 2 : 1));
+  static constexpr int kLanesPerHalf = 32 / kElem;  // lanes covering one 32-bit mask half
+};
+
+template <int E>
+__device__ __forceinline__ void load_vec_cg(const uint32_t* p, uint32_t* x) {
+  if constexpr (E == 4) {
+    const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p));
+    x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+  } else {
+    const uint2 v = __ldcg(reinterpret_cast<const uint2*>(p));
+    x[0] = v.x; x[1] = v.y;
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void load_vec(const uint32_t* p, uint32_t* x) {
+  if constexpr (E == 4) {
+    const uint4 v = *reinterpret_cast<const uint4*>(p);
+    x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+  } else {
+    const uint2 v = *reinterpret_cast<const uint2*>(p);
+    x[0] = v.x; x[1] = v.y;
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void store_vec(uint32_t* p, const uint32_t* x) {
+  if constexpr (E == 4) *reinterpret_cast<uint4*>(p) = make_uint4(x[0], x[1], x[2], x[3]);
+  else *reinterpret_cast<uint2*>(p) = make_uint2(x[0], x[1]);
+}
+
+// best[j] = min(best[j], relax(du[j], w)) for the lane's slots.
+template <int WK, int N>
+__device__ __forceinline__ void relax_min_row(uint32_t (&best)[N], const uint32_t* du,
+                                              uint32_t wbits) {
+  if constexpr (WK == kWeightF32) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) best[j] = min(best[j], gather_relax<WK>(du[j], wbits));
+  } else {
+    const uint32_t wt = (WK == kWeightU32) ? wbits : 1u;
+    const uint32_t lim = ~wt;
+#pragma unroll
+    for (int j = 0; j < N; ++j) best[j] = min(best[j], min(du[j], lim) + wt);
+  }
+}
+
+// Lane masks for the vectorised gather: bit r of *parts: the lane's vector of
+// part r lies inside the row (slot < Qg); bit j of *slots: slot j of the lane
+// is an SSSP slot.
+template <int W>
+__device__ __forceinline__ void gather_vec_masks(const LevelCtl* ctl, int Qg, int lane,
+                                                 uint32_t* parts, uint32_t* slots) {
+  using GV = GatherVec<W>;
+  uint32_t pm = 0, sm = 0;
+#pragma unroll
+  for (int r = 0; r < GV::kParts; ++r) {
+    const int base = (32 * r + lane) * GV::kElem;
+    if (base < Qg) pm |= 1u << r;
+#pragma unroll
+    for (int k = 0; k < GV::kElem; ++k) {
+      const int q = base + k;
+      if (q < Qg && ((ctl->sssp_bits[q >> 6] >> (q & 63)) & 1ULL)) sm |= 1u << (r * GV::kElem + k);
+    }
+  }
+  *parts = pm;
+  *slots = sm;
+}
+
+// ORs the lanes' per-slot bits into 64-bit frontier words: `bits` holds the
+// lane's kSlots bits (slot r*kElem + k at bit r*kElem + k).  For each part,
+// the lane whose slots start a word receives it in words[r] (0 elsewhere).
+template <int W>
+__device__ __forceinline__ void gather_vec_words(uint32_t bits, int lane,
+                                                 uint64_t (&words)[GatherVec<W>::kParts]) {
+  using GV = GatherVec<W>;
+  constexpr int E = GV::kElem;
+  constexpr int L = GV::kLanesPerHalf;
+#pragma unroll
+  for (int r = 0; r < GV::kParts; ++r) {
+    uint32_t h = ((bits >> (r * E)) & ((1u << E) - 1u)) << (E * (lane % L));
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) h |= __shfl_xor_sync(kFull, h, o);
+    const uint32_t hi = __shfl_down_sync(kFull, h, L);
+    words[r] = (lane % (2 * L) == 0) ? (static_cast<uint64_t>(hi) << 32) | h : 0ULL;
+  }
+}
+
+// Gathers in-edges [eb, ee) into best[] (vector layout).  `stage` is this
+// warp's 32-entry shared staging array.  All lanes call.
+template <int W, int WK>
+__device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGraph& G,
+                                                 const LevelView& lv, const uint64_t* sb,
+                                                 uint32_t pmask, int64_t eb, int64_t ee,
+                                                 int lane, int2* stage,
+                                                 uint32_t (&best)[GatherVec<W>::kSlots],
+                                                 unsigned long long& pairs,
+                                                 unsigned& scanned) {
+  using GV = GatherVec<W>;
+  constexpr int E = GV::kElem;
+  constexpr int P = GV::kParts;
+  constexpr int S = GV::kSteps;
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  const uint32_t* lanebase = g.values + lane * E;
+  for (int64_t e0 = eb; e0 < ee; e0 += 32) {
+    const int64_t e = e0 + lane;
+    int k = 0;
+    int32_t u = 0;
+    uint32_t wb = 0;
+    if (e < ee) {
+      u = G.pcol[e];
+      wb = weight_bits<WK>(G.pw, e);
+      uint64_t m[W];
+      load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
+#pragma unroll
+      for (int i = 0; i < W; ++i) k += __popcll(m[i] & sb[i]);
+      ++scanned;
+    }
+    pairs += static_cast<unsigned long long>(k);
+    const unsigned lm = __ballot_sync(kFull, k > 0);
+    if (k > 0) stage[__popc(lm & ((1u << lane) - 1u))] = make_int2(u, static_cast<int>(wb));
+    __syncwarp();
+    const int n = __popc(lm);
+    int i = 0;
+    for (; i + S <= n; i += S) {
+      int2 ed[S];
+#pragma unroll
+      for (int t = 0; t < S; ++t) ed[t] = stage[i + t];
+      uint32_t cur[S][GV::kSlots];
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
+#pragma unroll
+        for (int r = 0; r < P; ++r) {
+          if ((pmask >> r) & 1u) {
+            load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < E; ++q) cur[t][r * E + q] = 0xffffffffu;
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < S; ++t) relax_min_row<WK>(best, cur[t], static_cast<uint32_t>(ed[t].y));
+    }
+    for (; i < n; ++i) {
+      const int2 ed = stage[i];
+      const uint32_t* row = lanebase + static_cast<size_t>(ed.x) * Qg;
+      uint32_t cur[GV::kSlots];
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        if ((pmask >> r) & 1u) {
+          load_vec_cg<E>(row + 32 * E * r, &cur[r * E]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < E; ++q) cur[r * E + q] = 0xffffffffu;
+        }
+      }
+      relax_min_row<WK>(best, cur, static_cast<uint32_t>(ed.y));
+    }
+    __syncwarp();
+  }
+}
+
+// Gather level (vectorised), vertices of in-degree <= heavy_degree.
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sssp_pull_vec(GroupDev g, DevGraph G) {
+  using GV = GatherVec<W>;
+  constexpr int E = GV::kElem;
+  constexpr int P = GV::kParts;
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->sdir != kDirPull) return;
+  __shared__ int2 s_stage[kWarpsPerBlock][32];
+  const LevelView lv = level_view(g);
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const uint64_t* sb = ctl->sssp_bits;
+  uint32_t pmask, smask;
+  gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
+  const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  uint32_t uacc = 0;
+  unsigned long long improved = 0, pairs = 0;
+  unsigned scanned = 0, verts = 0;
+  for (unsigned long long vv = gw; vv < static_cast<unsigned long long>(G.V); vv += nwarps) {
+    const int32_t v = static_cast<int32_t>(vv);
+    const int64_t beg = row_at<OT>(G.prow, v);
+    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+    if (end == beg || end - beg > G.heavy_degree) continue;
+    ++verts;
+    uint32_t* row = g.values + static_cast<size_t>(v) * Qg + lane * E;
+    uint32_t best[GV::kSlots];
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      if ((pmask >> r) & 1u) {
+        load_vec<E>(row + 32 * E * r, &best[r * E]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < E; ++q) best[r * E + q] = 0u;
+      }
+    }
+    gather_edges_vec<W, WK>(g, G, lv, sb, pmask, beg, end, lane, s_stage[wib], best, pairs,
+                            scanned);
+    // commit (the warp owns v's row this level: the row read above is current)
+    uint32_t imp = 0;
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      if (!((pmask >> r) & 1u)) continue;
+      uint32_t o[E], nv[E];
+      load_vec<E>(row + 32 * E * r, o);
+      uint32_t b = 0;
+#pragma unroll
+      for (int q = 0; q < E; ++q) {
+        const int j = r * E + q;
+        const bool up = ((smask >> j) & 1u) && best[j] < o[q];
+        nv[q] = up ? best[j] : o[q];
+        b |= static_cast<uint32_t>(up) << q;
+      }
+      if (b) store_vec<E>(row + 32 * E * r, nv);
+      imp |= b << (r * E);
+    }
+    if (!__any_sync(kFull, imp != 0)) continue;
+    improved += __popc(imp);
+    uacc |= imp;
+    uint64_t words[P];
+    gather_vec_words<W>(imp, lane, words);
+#pragma unroll
+    for (int r = 0; r < P; ++r) {
+      if (words[r]) {
+        const int wi = ((32 * r + lane) * E) >> 6;
+        atomic_or64(lv.fnext + static_cast<size_t>(v) * W + wi, words[r]);
+      }
+    }
+    bool app = false;
+    if (lane == 0) app = atomicMax(g.stamp + v, lv.level + 1) < lv.level + 1;
+    warp_append(app, v, app ? degree_of<OT>(G.row, v) : 0, lv.nlist, lv.ncount, lv.nedges, lane);
+  }
+  {
+    uint64_t words[P];
+    gather_vec_words<W>(uacc, lane, words);
+#pragma unroll
+    for (int r = 0; r < P; ++r)
+      if (words[r]) atomic_or64(lv.nactive + (((32 * r + lane) * E) >> 6), words[r]);
+  }
+  warp_add(improved, &g.ctl->lc.improved, lane);
+  warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);
+  warp_add(scanned, &g.ctl->lc.spull_edges, lane);
+  warp_add(verts, &g.ctl->lc.spull_vertices, lane);
+}
+
+// Gather level (vectorised), heavy vertices: CTA per 2048-edge chunk, warps
+// min-reduce their slices into shared memory, one atomicMin per slot.
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevGraph G) {
+  using GV = GatherVec<W>;
+  constexpr int E = GV::kElem;
+  constexpr int C = 2 * W;
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->sdir != kDirPull || G.n_pheavy == 0) return;
+  const LevelView lv = level_view(g);
+  __shared__ uint32_t s_best[C * 32];
+  __shared__ int2 s_stage[kWarpsPerBlock][32];
+  __shared__ int32_t s_h;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const uint64_t* sb = ctl->sssp_bits;
+  uint32_t pmask, smask;
+  gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
+  const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long improved = 0, pairs = 0;
+  unsigned scanned = 0;
+  for (int64_t ch = blockIdx.x; ch < G.pheavy_chunks; ch += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = G.n_pheavy - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (G.pheavy_chunk_start[mid] <= ch) lo = mid;
+        else hi = mid - 1;
+      }
+      s_h = lo;
+    }
+    for (int i = threadIdx.x; i < C * 32; i += blockDim.x) s_best[i] = 0xffffffffu;
+    __syncthreads();
+    const int h = s_h;
+    const int32_t v = G.pheavy[h];
+    const int64_t beg = row_at<OT>(G.prow, v);
+    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+    const int64_t cb = beg + (ch - G.pheavy_chunk_start[h]) * kHeavyChunk;
+    const int64_t ce = min(end, cb + kHeavyChunk);
+    if (threadIdx.x == 0 && ch == G.pheavy_chunk_start[h]) atomicAdd(&g.ctl->lc.spull_vertices, 1ULL);
+    const int64_t seg = (ce - cb + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int64_t wb = cb + wib * seg;
+    const int64_t we = min(ce, wb + seg);
+    uint32_t best[GV::kSlots];
+#pragma unroll
+    for (int j = 0; j < GV::kSlots; ++j) best[j] = 0xffffffffu;
+    gather_edges_vec<W, WK>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best, pairs, scanned);
+#pragma unroll
+    for (int j = 0; j < GV::kSlots; ++j) {
+      const int q = (32 * (j / E) + lane) * E + (j % E);
+      if (((smask >> j) & 1u) && best[j] != 0xffffffffu) atomicMin(&s_best[q], best[j]);
+    }
+    __syncthreads();
+    // commit: warp wib takes 32-slot chunks wib, wib + 8, ... (lane j <-> slot 32c + j)
+    bool any = false;
+    for (int c = wib; c < C; c += kWarpsPerBlock) {
+      const int q = 32 * c + lane;
+      bool imp = false;
+      if ((lsel >> c) & 1u) {
+        const uint32_t b = s_best[q];
+        uint32_t* p = g.values + static_cast<size_t>(v) * Qg + q;
+        if (b < *p) imp = b < atomicMin(p, b);
+      }
+      const unsigned m = __ballot_sync(kFull, imp);
+      if (m) {
+        any = true;
+        if (lane == 0) {
+          const uint64_t bits = static_cast<uint64_t>(m) << (32 * (c & 1));
+          atomic_or64(lv.fnext + static_cast<size_t>(v) * W + (c >> 1), bits);
+          uni[c >> 1] |= bits;
+          improved += __popc(m);
+        }
+      }
+    }
+    bool app = false;
+    if (any && lane == 0) app = atomicMax(g.stamp + v, lv.level + 1) < lv.level + 1;
+    warp_append(app, v, app ? degree_of<OT>(G.row, v) : 0, lv.nlist, lv.ncount, lv.nedges, lane);
+    __syncthreads();
+  }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(improved, &g.ctl->lc.improved, lane);
+  warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);
+  warp_add(scanned, &g.ctl->lc.spull_edges, lane);
+}
+
 // --------------------------------------------------------- level control
 __device__ __forceinline__ int32_t decide_dir(const LevelCtl* ctl, unsigned long long count,
                                               unsigned long long edges, bool has_bfs) {

@@ -129,7 +129,7 @@ typedef struct {
   uint64_t sssp_pull_vertices; /* vertices an SSSP gather level scanned                 */
   uint64_t sssp_pull_edges;  /* in-edges an SSSP gather level scanned                    */
   int32_t sssp_mode;         /* SSSP direction of the level: 0 push (scatter), 1 pull (gather) */
-  int32_t reserved;
+  float kernel_ms;           /* the level's kernel time when profile_kernels is set, else 0 */
 } cgp_level_profile;
 
 /* run_result_t scalars (result.hxx:49-66). */

@@ -385,9 +385,10 @@ def test_sssp_execution_knobs_do_not_change_results(rmat_u32, opts):
     dict(traversal_mode="pull", heavy_degree=16),
     dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.05, heavy_degree=32, mask_words=16),
 ])
-def test_sssp_gather_parity(rmat_u32, rmat_f32, grid_f32, opts):
+@pytest.mark.parametrize("nq", [62, 70, 72])  # vector rows (uint2 / uint4) and scalar rows
+def test_sssp_gather_parity(rmat_u32, rmat_f32, grid_f32, opts, nq):
     for g, graph in (rmat_u32, rmat_f32, grid_f32):
-        src = g.pick_sources(70, seed=31)
+        src = g.pick_sources(nq, seed=31)
         ref, _ = oracle.batch("sssp", g, src)
         r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
                           cgp.RunOptions(profile_iterations=True, **opts), layout="query")
@@ -467,3 +468,30 @@ def test_mixed_batch_with_sssp_gather(rmat_u32, ratio):
             np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source, 2))
         else:
             np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
+
+
+@pytest.mark.parametrize("layout", ["vertex", "query"])
+@pytest.mark.parametrize("order", ["blocks", "interleaved", "with_wcc"])
+def test_large_mixed_batch_split_by_kind(rmat_u32, layout, order):
+    """>= 64 BFS and >= 64 SSSP queries run as separate per-kind groups; the
+    host result blocks are copied while later groups traverse (contiguous
+    blocks) or in one copy at the end (interleaved kinds, WCC columns)."""
+    g, graph = rmat_u32
+    src = g.pick_sources(180, seed=48)
+    if order == "interleaved":
+        kinds = ["bfs" if i % 2 else "sssp" for i in range(180)]
+    else:
+        kinds = ["bfs"] * 100 + ["sssp"] * 80
+    descs = [cgp.QueryDescriptor(int(s), k) for s, k in zip(src, kinds)]
+    if order == "with_wcc":
+        descs.append(cgp.QueryDescriptor(0, "wcc"))
+    r = cgp.run_heterogeneous(graph, cgp.HybridQueryBatch(descs), layout=layout)
+    assert r.groups == 2
+    vals = r.values if layout == "query" else r.values.T
+    for i, d in enumerate(descs):
+        if d.kind == "bfs":
+            np.testing.assert_array_equal(vals[i].view(np.int32), oracle.bfs(g, d.source))
+        elif d.kind == "sssp":
+            np.testing.assert_array_equal(vals[i], oracle.sssp(g, d.source))
+        else:
+            np.testing.assert_array_equal(vals[i], oracle.wcc_components(g))
