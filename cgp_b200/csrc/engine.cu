@@ -616,9 +616,15 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
     int n = per_chunk;
     if (max_levels > 0) n = std::min(n, max_levels - enqueued);
     if (n <= 0) break;
-    double before = 0;
-    if (kt)
-      for (int c = 0; c < kNumClasses; ++c) before += kt->ms[c];
+    // level time = the level kernels' classes (the open init interval of the
+    // group is charged to its own class when the first level's marks flush)
+    auto level_sum = [](const KernelTimer* t) {
+      double x = 0;
+      for (int c = 0; c < kNumClasses; ++c)
+        if (c != kClassInit && c != kClassOutput && c != kClassWcc) x += t->ms[c];
+      return x;
+    };
+    const double before = kt ? level_sum(kt) : 0.0;
     spec.launches += enqueue_levels(g, ws, spec, o, s, n, kt);
     enqueued += n;
     ck(cudaMemcpyAsync(&snap[chunk & 1], ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost, s),
@@ -628,9 +634,7 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
     if (kt) {
       kt->flush();
       ck(cudaEventSynchronize(ws->ev[chunk & 1]), "sync level");
-      double after = 0;
-      for (int c = 0; c < kNumClasses; ++c) after += kt->ms[c];
-      out->level_ms.push_back(static_cast<float>(after - before));
+      out->level_ms.push_back(static_cast<float>(level_sum(kt) - before));
       stop = snap[chunk & 1].done != 0;
     } else if (chunk > 0) {
       ck(cudaEventSynchronize(ws->ev[(chunk - 1) & 1]), "sync chunk");

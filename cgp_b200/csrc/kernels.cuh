@@ -1426,6 +1426,21 @@ __device__ __forceinline__ void gather_vec_words(uint32_t bits, int lane,
   }
 }
 
+// Whether the gather screens in-edges by their source's frontier mask: -1
+// when the frontier's out-edges are less than half of all edges; otherwise
+// the number of SSSP slots (every source is then read, which skips a
+// dependent mask load per 32 in-edges and costs little: almost every edge's
+// source is live).
+template <int W>
+__device__ __forceinline__ int gather_screen_qs(const LevelCtl* ctl, const LevelView& lv,
+                                                int64_t E) {
+  if (2 * ctl->edges[lv.par] < static_cast<unsigned long long>(E)) return -1;
+  int qs = 0;
+#pragma unroll
+  for (int i = 0; i < W; ++i) qs += __popcll(ctl->sssp_bits[i]);
+  return qs;
+}
+
 // Gathers in-edges [eb, ee) into best[] (vector layout).  `stage` is this
 // warp's 32-entry shared staging array.  All lanes call.
 template <int W, int WK>
@@ -1435,7 +1450,7 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
                                                  int lane, int2* stage,
                                                  uint32_t (&best)[GatherVec<W>::kSlots],
                                                  unsigned long long& pairs,
-                                                 unsigned& scanned) {
+                                                 unsigned& scanned, int screen_qs) {
   using GV = GatherVec<W>;
   constexpr int E = GV::kElem;
   constexpr int P = GV::kParts;
@@ -1450,10 +1465,15 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
     if (e < ee) {
       u = G.pcol[e];
       wb = weight_bits<WK>(G.pw, e);
-      uint64_t m[W];
-      load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
+      if (screen_qs < 0) {
+        // sparse frontier: skip in-edges whose source has no SSSP frontier bit
+        uint64_t m[W];
+        load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
 #pragma unroll
-      for (int i = 0; i < W; ++i) k += __popcll(m[i] & sb[i]);
+        for (int i = 0; i < W; ++i) k += __popcll(m[i] & sb[i]);
+      } else {
+        k = screen_qs;  // dense frontier: every in-edge is gathered (no mask load)
+      }
       ++scanned;
     }
     pairs += static_cast<unsigned long long>(k);
@@ -1523,10 +1543,21 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   uint32_t uacc = 0;
   unsigned long long improved = 0, pairs = 0;
   unsigned scanned = 0, verts = 0;
-  for (unsigned long long vv = gw; vv < static_cast<unsigned long long>(G.V); vv += nwarps) {
+  const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const unsigned long long V = static_cast<unsigned long long>(G.V);
+  // the next vertex's offsets are loaded while the current one is gathered
+  int64_t nbeg = 0, nend = 0;
+  if (gw < V) {
+    nbeg = row_at<OT>(G.prow, static_cast<int64_t>(gw));
+    nend = row_at<OT>(G.prow, static_cast<int64_t>(gw) + 1);
+  }
+  for (unsigned long long vv = gw; vv < V; vv += nwarps) {
     const int32_t v = static_cast<int32_t>(vv);
-    const int64_t beg = row_at<OT>(G.prow, v);
-    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+    const int64_t beg = nbeg, end = nend;
+    if (vv + nwarps < V) {
+      nbeg = row_at<OT>(G.prow, static_cast<int64_t>(vv + nwarps));
+      nend = row_at<OT>(G.prow, static_cast<int64_t>(vv + nwarps) + 1);
+    }
     if (end == beg || end - beg > G.heavy_degree) continue;
     ++verts;
     uint32_t* row = g.values + static_cast<size_t>(v) * Qg + lane * E;
@@ -1541,7 +1572,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
       }
     }
     gather_edges_vec<W, WK>(g, G, lv, sb, pmask, beg, end, lane, s_stage[wib], best, pairs,
-                            scanned);
+                            scanned, screen_qs);
     // commit (the warp owns v's row this level: the row read above is current)
     uint32_t imp = 0;
 #pragma unroll
@@ -1608,6 +1639,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   uint32_t pmask, smask;
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
+  const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
   const size_t Qg = static_cast<size_t>(g.Qg);
   uint64_t uni[W];
 #pragma unroll
@@ -1639,7 +1671,8 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
     uint32_t best[GV::kSlots];
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) best[j] = 0xffffffffu;
-    gather_edges_vec<W, WK>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best, pairs, scanned);
+    gather_edges_vec<W, WK>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best, pairs, scanned,
+                            screen_qs);
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) {
       const int q = (32 * (j / E) + lane) * E + (j % E);

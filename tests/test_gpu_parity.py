@@ -495,3 +495,36 @@ def test_large_mixed_batch_split_by_kind(rmat_u32, layout, order):
             np.testing.assert_array_equal(vals[i], oracle.sssp(g, d.source))
         else:
             np.testing.assert_array_equal(vals[i], oracle.wcc_components(g))
+
+
+@pytest.mark.parametrize("wrange", [(1, 64), (500, 4000), (1 << 20, 1 << 21), (1 << 30, 3 << 30)])
+@pytest.mark.parametrize("opts", [dict(traversal_mode="pull"),
+                                  dict(sssp_pull_edge_ratio=0.05, heavy_degree=32)])
+def test_sssp_gather_weight_ranges(wrange, opts):
+    """256-slot vector gathers with small, medium, large and near-overflow
+    integer weights (sums saturate at UINT32_MAX exactly like the oracle's)."""
+    g = cgp.gen_rmat(12, 8, seed=121).with_weights("u32", wrange[0], wrange[1], seed=122)
+    graph = cgp.CsrGraph(g)
+    src = g.pick_sources(256, seed=123)
+    ref, _ = oracle.batch("sssp", g, src)
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                      cgp.RunOptions(**opts), layout="query")
+    assert r.mask_words == 4
+    np.testing.assert_array_equal(r.values, ref)
+
+
+def test_sssp_gather_mixed_group(rmat_u32):
+    """A 256-slot group with 32 BFS slots: the gathers read whole rows, BFS
+    depths included, and must update only the SSSP slots."""
+    g, graph = rmat_u32
+    src = g.pick_sources(256, seed=124)
+    descs = [cgp.QueryDescriptor(int(s), "bfs" if i % 8 == 0 else "sssp")
+             for i, s in enumerate(src)]
+    r = cgp.run_heterogeneous(graph, cgp.HybridQueryBatch(descs),
+                              options=cgp.RunOptions(traversal_mode="pull"), layout="query")
+    assert r.groups == 1
+    for i, d in enumerate(descs):
+        if d.kind == "bfs":
+            np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source))
+        else:
+            np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
