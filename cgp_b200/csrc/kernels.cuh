@@ -723,9 +723,14 @@ __device__ __forceinline__ bool sssp_relax(const GroupDev& g, const LevelView& l
   const uint32_t old = atomicMin(dst, cand);
   if (cand >= old) return false;
   const uint64_t bit = 1ULL << (q & 63);
-  atomic_or64(lv.fnext + static_cast<size_t>(n) * W + (q >> 6), bit);
+  // hub destinations receive many improvements per level: a plain read of
+  // the frontier word and of the stamp skips atomics that would change
+  // nothing (bits and stamps only grow within a level)
+  uint64_t* fw = lv.fnext + static_cast<size_t>(n) * W + (q >> 6);
+  if (!(*fw & bit)) atomic_or64(fw, bit);
   uni[q >> 6] |= bit;
   ++improved;
+  if (g.stamp[n] >= lv.level + 1) return false;
   return atomicMax(g.stamp + n, lv.level + 1) < lv.level + 1;
 }
 
@@ -832,7 +837,8 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
           }
         }
         bool app = false;
-        if (any && lane == 0) app = atomicMax(g.stamp + nb, lv.level + 1) < lv.level + 1;
+        if (any && lane == 0 && g.stamp[nb] < lv.level + 1)
+          app = atomicMax(g.stamp + nb, lv.level + 1) < lv.level + 1;
         warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist, lv.ncount, lv.nedges,
                     lane);
       }
@@ -1503,20 +1509,28 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
 #pragma unroll
       for (int t = 0; t < S; ++t) relax_min_row<WK>(best, cur[t], static_cast<uint32_t>(ed[t].y));
     }
-    for (; i < n; ++i) {
-      const int2 ed = stage[i];
-      const uint32_t* row = lanebase + static_cast<size_t>(ed.x) * Qg;
-      uint32_t cur[GV::kSlots];
+    if (i < n) {
+      // the remaining 1..S-1 edges in one step (uniform predicates), so that
+      // a short list costs one round trip instead of one per edge
+      int2 ed[S];
 #pragma unroll
-      for (int r = 0; r < P; ++r) {
-        if ((pmask >> r) & 1u) {
-          load_vec_cg<E>(row + 32 * E * r, &cur[r * E]);
-        } else {
+      for (int t = 0; t < S; ++t) ed[t] = stage[i + t < n ? i + t : i];
+      uint32_t cur[S][GV::kSlots];
 #pragma unroll
-          for (int q = 0; q < E; ++q) cur[r * E + q] = 0xffffffffu;
+      for (int t = 0; t < S; ++t) {
+        const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
+#pragma unroll
+        for (int r = 0; r < P; ++r) {
+          if (i + t < n && ((pmask >> r) & 1u)) {
+            load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < E; ++q) cur[t][r * E + q] = 0xffffffffu;
+          }
         }
       }
-      relax_min_row<WK>(best, cur, static_cast<uint32_t>(ed.y));
+#pragma unroll
+      for (int t = 0; t < S; ++t) relax_min_row<WK>(best, cur[t], static_cast<uint32_t>(ed[t].y));
     }
     __syncwarp();
   }
