@@ -1536,6 +1536,23 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
   }
 }
 
+// Appends the n vertices buffered in lanes 0..n-1 to the next frontier list
+// with one reservation (all lanes call).
+template <typename OT>
+__device__ __forceinline__ void flush_appends(int32_t v, int n, const DevGraph& G,
+                                              const LevelView& lv, int lane) {
+  unsigned long long e = lane < n ? degree_of<OT>(G.row, v) : 0ULL;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(kFull, e, o);
+  unsigned long long base = 0;
+  if (lane == 0) {
+    base = atomicAdd(lv.ncount, static_cast<unsigned long long>(n));
+    atomicAdd(lv.nedges, e);
+  }
+  base = __shfl_sync(kFull, base, 0);
+  if (lane < n) lv.nlist[base + lane] = v;
+}
+
 // Gather level (vectorised), vertices of in-degree <= heavy_degree.
 template <int W, typename OT, int WK>
 __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sssp_pull_vec(GroupDev g, DevGraph G) {
@@ -1557,6 +1574,8 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   uint32_t uacc = 0;
   unsigned long long improved = 0, pairs = 0;
   unsigned scanned = 0, verts = 0;
+  int32_t pend_v = 0;  // lane i: i-th vertex waiting to be appended
+  int pend_n = 0;      // uniform
   const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
   const unsigned long long V = static_cast<unsigned long long>(G.V);
   // the next vertex's offsets are loaded while the current one is gathered
@@ -1610,17 +1629,28 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
     uacc |= imp;
     uint64_t words[P];
     gather_vec_words<W>(imp, lane, words);
+    // v is this warp's alone during the kernel (earlier kernels of the level
+    // are complete, heavy vertices are not in this kernel): its frontier
+    // words and stamp need no atomics
 #pragma unroll
     for (int r = 0; r < P; ++r) {
       if (words[r]) {
         const int wi = ((32 * r + lane) * E) >> 6;
-        atomic_or64(lv.fnext + static_cast<size_t>(v) * W + wi, words[r]);
+        lv.fnext[static_cast<size_t>(v) * W + wi] |= words[r];
       }
     }
-    bool app = false;
-    if (lane == 0) app = atomicMax(g.stamp + v, lv.level + 1) < lv.level + 1;
-    warp_append(app, v, app ? degree_of<OT>(G.row, v) : 0, lv.nlist, lv.ncount, lv.nedges, lane);
+    if (g.stamp[v] < lv.level + 1) {  // uniform: every lane reads the same word
+      __syncwarp();
+      if (lane == 0) g.stamp[v] = lv.level + 1;
+      // appends are buffered in the lanes and reserved 32 at a time
+      if (lane == pend_n) pend_v = v;
+      if (++pend_n == 32) {
+        flush_appends<OT>(pend_v, pend_n, G, lv, lane);
+        pend_n = 0;
+      }
+    }
   }
+  if (pend_n > 0) flush_appends<OT>(pend_v, pend_n, G, lv, lane);
   {
     uint64_t words[P];
     gather_vec_words<W>(uacc, lane, words);
