@@ -163,7 +163,9 @@ def level_bytes(p, kind, V, W, ob=4, qs=0):
     BFS pull: 2 V Wb + P 2o + S(4+Wb) + 4N
     SSSP push (scatter): U(2o+Wb+4) + D(4+4+Wb) + 4 sum(popc) + 8 A + Wb U'
     SSSP pull (gather):  2o V + 4 Qs P + S(4+4+Wb) + 4 A + 4 I + Wb U'
-    (A = (edge, active query) pairs, I = improved entries, Qs = SSSP slots)"""
+    (A = (edge, active query) pairs; on gather levels whose frontier holds half
+    of the edges or more every SSSP slot of every in-edge's source is read, and
+    A counts those pairs; I = improved entries, Qs = SSSP slots)"""
     Wb = 8 * W
     U, D, N, Un = p.frontier_size, p.frontier_edges, p.new_pairs, p.next_size
     if kind == "bfs":

@@ -85,6 +85,7 @@ struct LevelCtl {
   unsigned long long pull_edge_threshold;
   unsigned long long sssp_pull_edge_threshold;  // gather when frontier edges reach it
   unsigned long long dense_count;  // SSSP vertices queued for the dense kernel this level
+  unsigned long long hq_packed;    // heavy frontier queue: count << 40 | chunks, this level
   LevelCounters lc;                // counters of the current level
   LevelCounters total;             // sums over all levels
 };
@@ -128,6 +129,8 @@ struct GroupDev {
   uint32_t* values;    // [V*Qg] vertex-major values (SSSP, direct depths)
   uint64_t* hacc;      // [n_pheavy*W] pull accumulators of heavy vertices
   int32_t* dense_list; // [V] SSSP frontier vertices with many active bits
+  int32_t* hq_vertex;  // [n_heavy] heavy vertices of the current frontier
+  int64_t* hq_start;   // [n_heavy] their first chunk in the level's chunk space
   LevelCtl* ctl;
   LevelProfile* prof;
   const SlotDev* slots;

@@ -303,6 +303,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
   if (kt) kt->mark(kClassClear, s);
   k_clear_next<W><<<c, kBlock, 0, s>>>(L.g);
   ++n;
+  if (L.G.n_heavy) {
+    k_heavy_queue<OT><<<c, kBlock, 0, s>>>(L.g, L.G);
+    ++n;
+  }
   if (L.has_bfs) {
     if (kt) kt->mark(kClassBfsPush, s);
     k_bfs_push<W, OT, DEPTH><<<t, kBlock, 0, s>>>(L.g, L.G);
@@ -448,6 +452,8 @@ GroupDev group_dev(Workspace* ws, const GroupSpec& spec, bool profiles) {
                  : (spec.external_values ? spec.external_values : ws->values.as<uint32_t>());
   g.hacc = ws->hacc.as<uint64_t>();
   g.dense_list = ws->dense.as<int32_t>();
+  g.hq_vertex = ws->hq_vertex.as<int32_t>();
+  g.hq_start = ws->hq_start.as<int64_t>();
   g.ctl = ws->ctl.as<LevelCtl>();
   g.prof = profiles ? ws->prof.as<LevelProfile>() : nullptr;
   g.slots = ws->slots.as<SlotDev>();
@@ -481,6 +487,8 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   moved |= ws->list1.ensure(static_cast<size_t>(V) * 4);
   moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
   moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8);
+  moved |= ws->hq_vertex.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 4);
+  moved |= ws->hq_start.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 8);
   if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
   if (spec.depth_mode == kDepthPlanes) {
     moved |= ws->planes.ensure(static_cast<size_t>(kInitialPlanes) * mask_bytes);

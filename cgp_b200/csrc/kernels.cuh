@@ -261,6 +261,54 @@ __device__ __forceinline__ uint64_t degree_of(const void* row, int32_t v) {
   return static_cast<uint64_t>(row_at<OT>(row, v + 1) - row_at<OT>(row, v));
 }
 
+// Appends the n vertices buffered in lanes 0..n-1 to the next frontier list
+// with one reservation, adding their out-degrees to the edge counter (all
+// lanes call).
+template <typename OT>
+__device__ __forceinline__ void flush_appends(int32_t v, int n, const DevGraph& G,
+                                              const LevelView& lv, int lane) {
+  unsigned long long e = lane < n ? degree_of<OT>(G.row, v) : 0ULL;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(kFull, e, o);
+  unsigned long long base = 0;
+  if (lane == 0) {
+    base = atomicAdd(lv.ncount, static_cast<unsigned long long>(n));
+    atomicAdd(lv.nedges, e);
+  }
+  base = __shfl_sync(kFull, base, 0);
+  if (lane < n) lv.nlist[base + lane] = v;
+}
+
+// Per-warp buffer of vertices to append to the next frontier: lane i holds
+// the i-th, and a reservation on the list's shared counters is made once per
+// 32 vertices instead of once per step (those two counters are the most
+// contended words of a level).  All lanes call add() and flush().
+struct WarpAppender {
+  int32_t v = 0;  // lane i: pending vertex i
+  int n = 0;      // pending count (uniform)
+
+  template <typename OT>
+  __device__ __forceinline__ void add(bool pred, int32_t x, const DevGraph& G,
+                                      const LevelView& lv, int lane) {
+    const unsigned m = __ballot_sync(kFull, pred);
+    if (m == 0) return;
+    const int c = __popc(m);
+    if (n + c > 32) flush<OT>(G, lv, lane);
+    const int k = lane - n;  // this lane receives the k-th appended vertex
+    const bool take = k >= 0 && k < c;
+    const int src = take ? select_bit64(m, k) : lane;
+    const int32_t got = __shfl_sync(kFull, x, src);
+    if (take) v = got;
+    n += c;
+  }
+
+  template <typename OT>
+  __device__ __forceinline__ void flush(const DevGraph& G, const LevelView& lv, int lane) {
+    if (n > 0) flush_appends<OT>(v, n, G, lv, lane);
+    n = 0;
+  }
+};
+
 // Push level, non-heavy frontier vertices: one warp per tile of 32 list
 // entries; vertices with degree > 32 are expanded by the whole warp one at a
 // time, smaller ones edge-balanced across the warp through a warp scan.
@@ -269,6 +317,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->dir != kDirPush) return;
   const LevelView lv = level_view(g);
+  WarpAppender ap;
   const unsigned long long n = ctl->count[lv.par];
   uint64_t sel[W];
 #pragma unroll
@@ -322,8 +371,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
           nb = G.col[e];
           app = bfs_visit<W, DEPTH>(g, G.V, lv, nb, bf, uni, pairs);
         }
-        warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
-                    lv.ncount, lv.nedges, lane);
+        ap.add<OT>(app, nb, G, lv, lane);
       }
     }
 
@@ -360,13 +408,52 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
         nb = G.col[e];
         app = bfs_visit<W, DEPTH>(g, G.V, lv, nb, of, uni, pairs);
       }
-      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
-                  lv.ncount, lv.nedges, lane);
+      ap.add<OT>(app, nb, G, lv, lane);
     }
     __syncwarp();
   }
+  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(pairs, &g.ctl->lc.new_pairs, lane);
+}
+
+// Heavy frontier queue.  At the start of a push level the frontier list is
+// scanned once and every vertex of degree > heavy_degree is queued with its
+// range of kHeavyChunk-edge chunks; one 64-bit atomicAdd hands out both the
+// queue slot (high bits) and the first chunk (low bits), so chunk starts grow
+// with the slot and a chunk finds its vertex by binary search.  The heavy
+// push kernels then visit only the heavy vertices of this frontier instead of
+// every heavy vertex of the graph.
+constexpr int kQueueShift = 40;
+
+template <typename OT>
+__global__ void __launch_bounds__(kBlock) k_heavy_queue(GroupDev g, DevGraph G) {
+  LevelCtl* ctl = g.ctl;
+  if (ctl->done || (ctl->dir != kDirPush && ctl->sdir != kDirPush)) return;
+  const LevelView lv = level_view(g);
+  const unsigned long long n = ctl->count[lv.par];
+  for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+       i < n; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const int32_t u = lv.list[i];
+    const int64_t deg = row_at<OT>(G.row, static_cast<int64_t>(u) + 1) - row_at<OT>(G.row, u);
+    if (deg <= G.heavy_degree) continue;
+    const unsigned long long chunks = static_cast<unsigned long long>((deg + kHeavyChunk - 1) / kHeavyChunk);
+    const unsigned long long old = atomicAdd(&ctl->hq_packed, (1ULL << kQueueShift) | chunks);
+    const unsigned long long slot = old >> kQueueShift;
+    g.hq_vertex[slot] = u;
+    g.hq_start[slot] = static_cast<int64_t>(old & ((1ULL << kQueueShift) - 1));
+  }
+}
+
+// Queue slot of chunk c (the last slot whose first chunk is <= c).
+__device__ __forceinline__ int heavy_queue_slot(const GroupDev& g, int nq, int64_t c) {
+  int lo = 0, hi = nq - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (g.hq_start[mid] <= c) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 
 // Push level, heavy frontier vertices: the static heavy list is cut into
@@ -374,28 +461,25 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
 template <int W, typename OT, int DEPTH>
 __global__ void __launch_bounds__(kBlock) k_bfs_push_heavy(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done || ctl->dir != kDirPush || G.n_heavy == 0) return;
+  if (ctl->done || ctl->dir != kDirPush) return;
+  const unsigned long long hq = ctl->hq_packed;
+  const int nq = static_cast<int>(hq >> kQueueShift);
+  const int64_t nchunks = static_cast<int64_t>(hq & ((1ULL << kQueueShift) - 1));
+  if (nq == 0) return;
   const LevelView lv = level_view(g);
+  WarpAppender ap;
   __shared__ int32_t s_h;
   const int lane = threadIdx.x & 31;
   uint64_t uni[W];
 #pragma unroll
   for (int i = 0; i < W; ++i) uni[i] = 0;
   unsigned long long pairs = 0;
-  for (int64_t c = blockIdx.x; c < G.heavy_chunks; c += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = G.n_heavy - 1;  // last h with start[h] <= c
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (G.heavy_chunk_start[mid] <= c) lo = mid;
-        else hi = mid - 1;
-      }
-      s_h = lo;
-    }
+  for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    if (threadIdx.x == 0) s_h = heavy_queue_slot(g, nq, c);
     __syncthreads();
     const int h = s_h;
     __syncthreads();
-    const int32_t u = G.heavy[h];
+    const int32_t u = g.hq_vertex[h];
     uint64_t f[W];
     load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, f);
 #pragma unroll
@@ -403,7 +487,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push_heavy(GroupDev g, DevGraph 
     if (!mask_any<W>(f)) continue;
     const int64_t beg = row_at<OT>(G.row, u);
     const int64_t end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
-    const int64_t cb = beg + (c - G.heavy_chunk_start[h]) * kHeavyChunk;
+    const int64_t cb = beg + (c - g.hq_start[h]) * kHeavyChunk;
     const int64_t ce = min(end, cb + kHeavyChunk);
     for (int64_t e0 = cb + (threadIdx.x & ~31); e0 < ce; e0 += blockDim.x) {
       const int64_t e = e0 + lane;
@@ -413,10 +497,10 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push_heavy(GroupDev g, DevGraph 
         nb = G.col[e];
         app = bfs_visit<W, DEPTH>(g, G.V, lv, nb, f, uni, pairs);
       }
-      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
-                  lv.ncount, lv.nedges, lane);
+      ap.add<OT>(app, nb, G, lv, lane);
     }
   }
+  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(pairs, &g.ctl->lc.new_pairs, lane);
 }
@@ -768,7 +852,8 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
                                                  const LevelView& lv, int32_t u,
                                                  const uint64_t (&bits)[W], int64_t eb,
                                                  int64_t ee, int lane, uint64_t (&uni)[W],
-                                                 unsigned long long& improved) {
+                                                 unsigned long long& improved,
+                                                 WarpAppender& ap) {
   const size_t Qg = static_cast<size_t>(g.Qg);
   uint32_t half[2 * W];
   uint32_t du[2 * W];
@@ -839,8 +924,7 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
         bool app = false;
         if (any && lane == 0 && g.stamp[nb] < lv.level + 1)
           app = atomicMax(g.stamp + nb, lv.level + 1) < lv.level + 1;
-        warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist, lv.ncount, lv.nedges,
-                    lane);
+        ap.add<OT>(app, nb, G, lv, lane);
       }
     }
   }
@@ -853,6 +937,7 @@ __global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDe
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->sdir != kDirPush) return;
   const LevelView lv = level_view(g);
+  WarpAppender ap;
   const unsigned long long n = ctl->dense_count;
   const int lane = threadIdx.x & 31;
   const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -869,8 +954,9 @@ __global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDe
     load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
 #pragma unroll
     for (int k = 0; k < W; ++k) b[k] &= ctl->sssp_bits[k];
-    sssp_dense_edges<W, OT, WK, U>(g, G, lv, u, b, beg, end, lane, uni, improved);
+    sssp_dense_edges<W, OT, WK, U>(g, G, lv, u, b, beg, end, lane, uni, improved, ap);
   }
+  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(improved, &g.ctl->lc.improved, lane);
 }
@@ -883,6 +969,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->sdir != kDirPush) return;
   const LevelView lv = level_view(g);
+  WarpAppender ap;
   const unsigned long long n = ctl->count[lv.par];
   uint64_t sel[W];
 #pragma unroll
@@ -974,11 +1061,11 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
         nb = G.col[e];
         app = sssp_relax<W, WK>(g, lv, s_u[wib][lo], nb, q, G.w, e, uni, improved);
       }
-      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
-                  lv.ncount, lv.nedges, lane);
+      ap.add<OT>(app, nb, G, lv, lane);
     }
     __syncwarp();
   }
+  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(improved, &g.ctl->lc.improved, lane);
   warp_add(spairs, &g.ctl->lc.sssp_pairs, lane);
@@ -990,8 +1077,13 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
 template <int W, typename OT, int WK>
 __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done || ctl->sdir != kDirPush || G.n_heavy == 0) return;
+  if (ctl->done || ctl->sdir != kDirPush) return;
+  const unsigned long long hq = ctl->hq_packed;
+  const int nq = static_cast<int>(hq >> kQueueShift);
+  const int64_t nchunks = static_cast<int64_t>(hq & ((1ULL << kQueueShift) - 1));
+  if (nq == 0) return;
   const LevelView lv = level_view(g);
+  WarpAppender ap;
   __shared__ int32_t s_h;
   __shared__ int32_t s_k;
   __shared__ int16_t s_q[kMaxW * 64];
@@ -1001,19 +1093,11 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
 #pragma unroll
   for (int i = 0; i < W; ++i) uni[i] = 0;
   unsigned long long improved = 0;
-  for (int64_t c = blockIdx.x; c < G.heavy_chunks; c += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = G.n_heavy - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (G.heavy_chunk_start[mid] <= c) lo = mid;
-        else hi = mid - 1;
-      }
-      s_h = lo;
-    }
+  for (int64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    if (threadIdx.x == 0) s_h = heavy_queue_slot(g, nq, c);
     __syncthreads();
     const int h = s_h;
-    const int32_t u = G.heavy[h];
+    const int32_t u = g.hq_vertex[h];
     uint64_t b[W];
     load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
 #pragma unroll
@@ -1037,17 +1121,17 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
       // each warp takes a contiguous slice of the chunk's edges
       const int64_t beg = row_at<OT>(G.row, u);
       const int64_t end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
-      const int64_t cb = beg + (c - G.heavy_chunk_start[h]) * kHeavyChunk;
+      const int64_t cb = beg + (c - g.hq_start[h]) * kHeavyChunk;
       const int64_t ce = min(end, cb + kHeavyChunk);
       if (threadIdx.x == 0) {
         atomicAdd(&g.ctl->lc.sssp_pairs, static_cast<unsigned long long>(ce - cb) * k);
-        if (c == G.heavy_chunk_start[h]) atomicAdd(&g.ctl->lc.sssp_active, static_cast<unsigned long long>(k));
+        if (c == g.hq_start[h]) atomicAdd(&g.ctl->lc.sssp_active, static_cast<unsigned long long>(k));
       }
       const int nw = blockDim.x >> 5;
       const int64_t seg = (ce - cb + nw - 1) / nw;
       const int64_t wb = cb + (threadIdx.x >> 5) * seg;
       const int64_t we = min(ce, wb + seg);
-      sssp_dense_edges<W, OT, WK, 1>(g, G, lv, u, b, wb, we, lane, uni, improved);
+      sssp_dense_edges<W, OT, WK, 1>(g, G, lv, u, b, wb, we, lane, uni, improved, ap);
       __syncthreads();
       continue;
     }
@@ -1059,12 +1143,12 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
     __syncthreads();
     const int64_t beg = row_at<OT>(G.row, u);
     const int64_t end = row_at<OT>(G.row, static_cast<int64_t>(u) + 1);
-    const int64_t cb = beg + (c - G.heavy_chunk_start[h]) * kHeavyChunk;
+    const int64_t cb = beg + (c - g.hq_start[h]) * kHeavyChunk;
     const int64_t ce = min(end, cb + kHeavyChunk);
     const long long pairs = static_cast<long long>(ce - cb) * k;
     if (threadIdx.x == 0) {
       atomicAdd(&g.ctl->lc.sssp_pairs, static_cast<unsigned long long>(pairs));
-      if (c == G.heavy_chunk_start[h]) atomicAdd(&g.ctl->lc.sssp_active, static_cast<unsigned long long>(k));
+      if (c == g.hq_start[h]) atomicAdd(&g.ctl->lc.sssp_active, static_cast<unsigned long long>(k));
     }
     for (long long p0 = threadIdx.x & ~31; p0 < pairs; p0 += blockDim.x) {
       const long long p = p0 + lane;
@@ -1077,11 +1161,11 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
         nb = G.col[e];
         app = sssp_relax<W, WK>(g, lv, u, nb, q, G.w, e, uni, improved);
       }
-      warp_append(app, nb, app ? degree_of<OT>(G.row, nb) : 0, lv.nlist,
-                  lv.ncount, lv.nedges, lane);
+      ap.add<OT>(app, nb, G, lv, lane);
     }
     __syncthreads();
   }
+  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(improved, &g.ctl->lc.improved, lane);
 }
@@ -1211,7 +1295,7 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 2)) k_sssp_pull(GroupDev
     const int64_t beg = row_at<OT>(G.prow, v);
     const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
     if (end == beg || end - beg > G.heavy_degree) continue;
-    ++verts;
+    if (lane == 0) ++verts;  // one count per vertex, not per lane
     uint32_t* row = g.values + static_cast<size_t>(v) * Qg + lane;
     uint32_t best[C];
 #pragma unroll
@@ -1536,22 +1620,6 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
   }
 }
 
-// Appends the n vertices buffered in lanes 0..n-1 to the next frontier list
-// with one reservation (all lanes call).
-template <typename OT>
-__device__ __forceinline__ void flush_appends(int32_t v, int n, const DevGraph& G,
-                                              const LevelView& lv, int lane) {
-  unsigned long long e = lane < n ? degree_of<OT>(G.row, v) : 0ULL;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(kFull, e, o);
-  unsigned long long base = 0;
-  if (lane == 0) {
-    base = atomicAdd(lv.ncount, static_cast<unsigned long long>(n));
-    atomicAdd(lv.nedges, e);
-  }
-  base = __shfl_sync(kFull, base, 0);
-  if (lane < n) lv.nlist[base + lane] = v;
-}
 
 // Gather level (vectorised), vertices of in-degree <= heavy_degree.
 template <int W, typename OT, int WK>
@@ -1592,7 +1660,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
       nend = row_at<OT>(G.prow, static_cast<int64_t>(vv + nwarps) + 1);
     }
     if (end == beg || end - beg > G.heavy_degree) continue;
-    ++verts;
+    if (lane == 0) ++verts;  // one count per vertex, not per lane
     uint32_t* row = g.values + static_cast<size_t>(v) * Qg + lane * E;
     uint32_t best[GV::kSlots];
 #pragma unroll
@@ -1674,6 +1742,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->sdir != kDirPull || G.n_pheavy == 0) return;
   const LevelView lv = level_view(g);
+  WarpAppender ap;
   __shared__ uint32_t s_best[C * 32];
   __shared__ int2 s_stage[kWarpsPerBlock][32];
   __shared__ int32_t s_h;
@@ -1746,9 +1815,10 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
     }
     bool app = false;
     if (any && lane == 0) app = atomicMax(g.stamp + v, lv.level + 1) < lv.level + 1;
-    warp_append(app, v, app ? degree_of<OT>(G.row, v) : 0, lv.nlist, lv.ncount, lv.nedges, lane);
+    ap.add<OT>(app, v, G, lv, lane);
     __syncthreads();
   }
+  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(improved, &g.ctl->lc.improved, lane);
   warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);
@@ -1833,6 +1903,7 @@ __global__ void k_level_end(GroupDev g) {
   ctl->total.spull_edges += ctl->lc.spull_edges;
   ctl->lc = LevelCounters{};
   ctl->dense_count = 0;
+  ctl->hq_packed = 0;
   ctl->total_frontier += ctl->count[par];
   ctl->total_edges += ctl->edges[par];
   if (ctl->dir == kDirPush) ctl->push_levels++;

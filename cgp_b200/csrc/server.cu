@@ -286,6 +286,8 @@ GroupDev server_dev(cgp_server* sv) {
   g.values = ws->values.as<uint32_t>();
   g.hacc = ws->hacc.as<uint64_t>();
   g.dense_list = ws->dense.as<int32_t>();
+  g.hq_vertex = nullptr;
+  g.hq_start = nullptr;
   g.ctl = ws->ctl.as<LevelCtl>();
   g.prof = nullptr;
   g.slots = ws->slots.as<SlotDev>();

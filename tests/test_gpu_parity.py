@@ -393,6 +393,9 @@ def test_sssp_gather_parity(rmat_u32, rmat_f32, grid_f32, opts, nq):
         r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
                           cgp.RunOptions(profile_iterations=True, **opts), layout="query")
         np.testing.assert_array_equal(r.values, ref)
+        for p in r.iteration_profiles:  # work counters are per vertex / per edge
+            assert p.sssp_pull_vertices <= g.num_vertices
+            assert p.sssp_pull_edges <= g.num_edges
         modes = {p.sssp_mode for p in r.iteration_profiles}
         if opts.get("sssp_pull_edge_ratio", 1) == 0.0:
             assert modes == {"push"}
