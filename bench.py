@@ -59,6 +59,8 @@ def parse_args():
     p.add_argument("--pull-frontier-ratio", type=float, default=0.15)
     p.add_argument("--heavy-degree", type=int, default=0)
     p.add_argument("--sssp-pull-edge-ratio", type=float, default=0.5)
+    p.add_argument("--no-light-chunks", action="store_true",
+                   help="gather light vertices one warp per vertex instead of in CTA chunks")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--json-out", default="")
     p.add_argument("--serve", action="store_true",
@@ -429,7 +431,8 @@ def main():
     stream = torch.cuda.current_stream(dev)
     tuning = dict(traversal_mode=args.mode, pull_edge_ratio=args.pull_edge_ratio,
                   pull_frontier_ratio=args.pull_frontier_ratio, heavy_degree=args.heavy_degree,
-                  sssp_pull_edge_ratio=args.sssp_pull_edge_ratio)
+                  sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
+                  light_chunks=not args.no_light_chunks)
     opts = cgp.RunOptions(stream=stream.cuda_stream, **tuning)
 
     empty = cgp.RunResult(values=None, iterations=0, gpu_time_ms=0.0, wall_time_ms=0.0)

@@ -38,7 +38,7 @@ class CgpOptions(Structure):
         ("use_cuda_graph", c_int32), ("levels_per_sync", c_int32), ("mask_words", c_int32),
         ("depth_mode", c_int32), ("heavy_degree", c_int32), ("max_queries", c_int32),
         ("discard_results", c_int32), ("profile_kernels", c_int32), ("dense_unroll", c_int32),
-        ("sssp_pull_edge_ratio", c_double), ("reserved", c_int32 * 2),
+        ("sssp_pull_edge_ratio", c_double), ("light_chunks", c_int32), ("reserved", c_int32),
         ("stream", c_void_p),
     ]
 

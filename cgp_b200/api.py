@@ -285,6 +285,7 @@ class RunOptions:
     profile_kernels: bool = False
     dense_unroll: int = 0
     sssp_pull_edge_ratio: float = 0.5
+    light_chunks: bool = True
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -307,6 +308,7 @@ class RunOptions:
         o.profile_kernels = int(self.profile_kernels)
         o.dense_unroll = self.dense_unroll
         o.sssp_pull_edge_ratio = self.sssp_pull_edge_ratio
+        o.light_chunks = 0 if self.light_chunks else -1
         o.stream = self.stream or None
         return o
 
@@ -446,7 +448,8 @@ def autotune(graph: CsrGraph, descs: Sequence[QueryDescriptor], options: RunOpti
                                pull_edge_ratio=o.pull_edge_ratio,
                                pull_frontier_ratio=o.pull_frontier_ratio,
                                dense_unroll=o.dense_unroll,
-                               sssp_pull_edge_ratio=o.sssp_pull_edge_ratio)
+                               sssp_pull_edge_ratio=o.sssp_pull_edge_ratio,
+                               light_chunks=o.light_chunks >= 0)
 
 
 def run(policy: str, graph: CsrGraph, queries, context=None, options: RunOptions | None = None,

@@ -15,6 +15,8 @@ constexpr int kWarpsPerBlock = kBlock / 32;
 constexpr int kHeavyChunk = 2048;  // edges of a heavy vertex per CTA work item
 constexpr int kMaxW = 16;
 constexpr int kMaxPlanes = 24;
+constexpr int kLightChunkVerts = 32;    // light vertices per chunked-gather CTA item
+constexpr int kLightChunkEdges = 2048;  // and their in-edges
 
 enum : int32_t { kDirPush = 0, kDirPull = 1 };
 enum : int32_t { kDepthNone = 0, kDepthDirect = 1, kDepthPlanes = 2 };
@@ -116,6 +118,9 @@ struct DevGraph {
   int32_t n_pheavy;
   int64_t pheavy_chunks;
   int64_t heavy_degree;
+  const int32_t* plight;             // light vertices of the pull CSR (chunked gathers)
+  const int32_t* plight_chunk_start; // [n_plight_chunks + 1]
+  int32_t n_plight_chunks;
 };
 
 struct GroupDev {

@@ -132,6 +132,9 @@ DevGraph GraphImpl::dev_graph(int64_t h) {
   d.pheavy_chunk_start = hp.pheavy.chunk_start.as<int64_t>();
   d.n_pheavy = hp.pheavy.n;
   d.pheavy_chunks = hp.pheavy.chunks;
+  d.plight = hp.plight.vertices.as<int32_t>();
+  d.plight_chunk_start = hp.plight.chunk_start.as<int32_t>();
+  d.n_plight_chunks = hp.plight.chunks;
   d.heavy_degree = h;
   return d;
 }
@@ -166,6 +169,35 @@ void build_heavy(const std::vector<int64_t>& row, int64_t V, int64_t h, HeavyTab
      "upload heavy chunks");
 }
 
+void build_light_chunks(const std::vector<int64_t>& row, int64_t V, int64_t h, LightChunks& t) {
+  std::vector<int32_t> vs;
+  std::vector<int32_t> cs{0};
+  int cur_v = 0;
+  int64_t cur_e = 0;
+  for (int64_t v = 0; v < V; ++v) {
+    const int64_t d = row[v + 1] - row[v];
+    if (d == 0 || d > h) continue;
+    if (cur_v > 0 && (cur_v == dev::kLightChunkVerts || cur_e + d > dev::kLightChunkEdges)) {
+      cs.push_back(static_cast<int32_t>(vs.size()));
+      cur_v = 0;
+      cur_e = 0;
+    }
+    vs.push_back(static_cast<int32_t>(v));
+    ++cur_v;
+    cur_e += d;
+  }
+  if (cur_v > 0) cs.push_back(static_cast<int32_t>(vs.size()));
+  t.n = static_cast<int32_t>(vs.size());
+  t.chunks = static_cast<int32_t>(cs.size()) - 1;
+  t.vertices.ensure(std::max<size_t>(vs.size(), 1) * sizeof(int32_t));
+  t.chunk_start.ensure(cs.size() * sizeof(int32_t));
+  if (!vs.empty())
+    ck(cudaMemcpy(t.vertices.p, vs.data(), vs.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+       "upload light vertices");
+  ck(cudaMemcpy(t.chunk_start.p, cs.data(), cs.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+     "upload light chunks");
+}
+
 }  // namespace
 
 const HeavyPair& GraphImpl::heavy_for(int64_t h) {
@@ -178,6 +210,7 @@ const HeavyPair& GraphImpl::heavy_for(int64_t h) {
     HostCsr& hc = g_host[this];
     build_heavy(hc.row, V, h, hp->heavy);
     build_heavy(hc.trow.empty() ? hc.row : hc.trow, V, h, hp->pheavy);
+    build_light_chunks(hc.trow.empty() ? hc.row : hc.trow, V, h, hp->plight);
   }
   return *heavy_cache.emplace(h, std::move(hp)).first->second;
 }
@@ -269,6 +302,7 @@ struct Grids {
   int gather_heavy;
   int gather_vec;
   int gather_heavy_vec;
+  int gather_chunked;
 };
 
 struct LevelLaunch {
@@ -280,6 +314,7 @@ struct LevelLaunch {
   bool pull;
   bool spull;        // SSSP gather kernels are part of the level
   bool gvec;         // rows allow the vectorised gather (alignment, width)
+  bool lchunks;      // light vertices gathered in CTA chunks (W <= 4)
   int dense_unroll;  // edges per step of the dense SSSP kernel (1 or 2)
   KernelTimer* kt;   // per-class event timing (non-graph runs only)
 };
@@ -342,7 +377,15 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
     }
     if (L.spull) {
       if (kt) kt->mark(kClassSsspPull, s);
-      if (L.gvec)
+      if constexpr (W <= 4) {
+        if (L.gvec && L.lchunks) {
+          k_sssp_pull_chunked<W, OT, WK><<<L.gr.gather_chunked, kBlock, 0, s>>>(L.g, L.G);
+        } else if (L.gvec) {
+          k_sssp_pull_vec<W, OT, WK><<<L.gr.gather_vec, kBlock, 0, s>>>(L.g, L.G);
+        } else {
+          k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
+        }
+      } else if (L.gvec)
         k_sssp_pull_vec<W, OT, WK><<<L.gr.gather_vec, kBlock, 0, s>>>(L.g, L.G);
       else
         k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
@@ -366,8 +409,9 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
 template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
   static int tile = 0, heavy = 0, dense = 0, dense2 = 0, gather = 0, gather_heavy = 0;
-  static int gather_vec = 0, gather_heavy_vec = 0;
+  static int gather_vec = 0, gather_heavy_vec = 0, gather_chunked = 0;
   if (tile == 0) {
+    if constexpr (W <= 4) gather_chunked = occupancy_grid(k_sssp_pull_chunked<W, OT, WK>, sms);
     gather_vec = occupancy_grid(k_sssp_pull_vec<W, OT, WK>, sms);
     gather_heavy_vec = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK>, sms);
     gather = occupancy_grid(k_sssp_pull<W, OT, WK>, sms);
@@ -391,6 +435,7 @@ Grids grids_t(int sms) {
   g.gather_heavy = gather_heavy;
   g.gather_vec = gather_vec;
   g.gather_heavy_vec = gather_heavy_vec;
+  g.gather_chunked = gather_chunked;
   return g;
 }
 
@@ -577,6 +622,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
     const int elem = spec.W == 1 ? 2 : 4;
     L.gvec = L.g.values != nullptr && spec.Qg % elem == 0 &&
              reinterpret_cast<uintptr_t>(L.g.values) % (4 * elem) == 0;
+    L.lchunks = spec.W <= 4 && o.light_chunks >= 0;
   }
   L.dense_unroll = o.dense_unroll == 2 ? 2 : 1;
   L.kt = kt;
@@ -590,7 +636,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   auto key = std::make_tuple(spec.W, g->offset_bytes, spec.depth_mode, g->weight_kind,
                              (spec.has_bfs ? 1 : 0) | (spec.has_sssp ? 2 : 0) | (L.pull ? 4 : 0) |
                                  (o.profile_iterations ? 8 : 0) | (L.dense_unroll == 2 ? 16 : 0) |
-                                 (L.spull ? 32 : 0),
+                                 (L.spull ? 32 : 0) | (L.lchunks ? 64 : 0),
                              levels, spec.Qg, static_cast<int>(L.G.heavy_degree), ws->generation,
                              reinterpret_cast<uint64_t>(L.g.values));
   auto it = ws->graphs.find(key);

@@ -1732,6 +1732,214 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   warp_add(verts, &g.ctl->lc.spull_vertices, lane);
 }
 
+// Gather level (vectorised), light vertices in CTA chunks.  A chunk is a
+// run of up to kLightChunkVerts light vertices with at most kLightChunkEdges
+// in-edges in total (static table of the pull CSR).  The CTA's warps split
+// the chunk's in-edges evenly, across vertex boundaries, so every warp keeps
+// several source rows in flight all the time instead of stalling on each
+// small vertex's chain of dependent loads; a warp min-reduces its run of one
+// vertex into that vertex's row in shared memory, and after a barrier each
+// vertex is committed once (compare, store, frontier words, append: no
+// atomics, the chunk owns its vertices).  W <= 4 (a row of 64W slots fits
+// 32 times in 32 KB of shared memory).
+template <int W, typename OT, int WK>
+__global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, DevGraph G) {
+  static_assert(W <= 4, "chunked gather holds 32 rows of at most 256 slots");
+  using GV = GatherVec<W>;
+  constexpr int E = GV::kElem;
+  constexpr int P = GV::kParts;
+  constexpr int S = GV::kSteps < 4 ? GV::kSteps : 4;
+  constexpr int R = 64 * W;
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->sdir != kDirPull || G.n_plight_chunks == 0) return;
+  const LevelView lv = level_view(g);
+  __shared__ __align__(16) uint32_t s_best[kLightChunkVerts * R];
+  __shared__ int4 s_stage[kWarpsPerBlock][32];
+  __shared__ int32_t s_v[kLightChunkVerts];
+  __shared__ int64_t s_beg[kLightChunkVerts];
+  __shared__ int32_t s_pre[kLightChunkVerts + 1];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const uint64_t* sb = ctl->sssp_bits;
+  uint32_t pmask, smask;
+  gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
+  const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const size_t Qg = static_cast<size_t>(g.Qg);
+  const uint32_t* lanebase = g.values + lane * E;
+  WarpAppender ap;
+  uint32_t uacc = 0;
+  unsigned long long improved = 0, pairs = 0;
+  unsigned scanned = 0, verts = 0;
+  for (int c = blockIdx.x; c < G.n_plight_chunks; c += gridDim.x) {
+    const int cs = G.plight_chunk_start[c];
+    const int nv = G.plight_chunk_start[c + 1] - cs;
+    if (wib == 0) {
+      int32_t v = 0;
+      int64_t b = 0;
+      int d = 0;
+      if (lane < nv) {
+        v = G.plight[cs + lane];
+        b = row_at<OT>(G.prow, v);
+        d = static_cast<int>(row_at<OT>(G.prow, static_cast<int64_t>(v) + 1) - b);
+      }
+      int inc = d;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += t;
+      }
+      if (lane < nv) {
+        s_v[lane] = v;
+        s_beg[lane] = b;
+        s_pre[lane + 1] = inc;
+      }
+      if (lane == 0) s_pre[0] = 0;
+    }
+    for (int i = threadIdx.x; i < nv * R; i += blockDim.x) s_best[i] = 0xffffffffu;
+    __syncthreads();
+    const int total = s_pre[nv];
+    const int seg = (total + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int fa = min(total, wib * seg);
+    const int fb = min(total, fa + seg);
+    uint32_t best[GV::kSlots];
+#pragma unroll
+    for (int j = 0; j < GV::kSlots; ++j) best[j] = 0xffffffffu;
+    int cur_k = -1;
+    // adds this warp's run of vertex cur_k into its shared row
+    auto flush_row = [&]() {
+      uint32_t* row = s_best + cur_k * R;
+#pragma unroll
+      for (int j = 0; j < GV::kSlots; ++j) {
+        if (best[j] != 0xffffffffu) atomicMin(row + (32 * (j / E) + lane) * E + (j % E), best[j]);
+        best[j] = 0xffffffffu;
+      }
+    };
+    int4* stage = s_stage[wib];
+    for (int f0 = fa; f0 < fb; f0 += 32) {
+      const int f = f0 + lane;
+      int cnt = 0, k = 0;
+      int32_t u = 0;
+      uint32_t wb = 0;
+      if (f < fb) {
+        int lo = 0, hi = nv - 1;  // owner: last k with s_pre[k] <= f
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_pre[mid] <= f) lo = mid;
+          else hi = mid - 1;
+        }
+        k = lo;
+        const int64_t e = s_beg[k] + (f - s_pre[k]);
+        u = G.pcol[e];
+        wb = weight_bits<WK>(G.pw, e);
+        if (screen_qs < 0) {
+          uint64_t m[W];
+          load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
+#pragma unroll
+          for (int i = 0; i < W; ++i) cnt += __popcll(m[i] & sb[i]);
+        } else {
+          cnt = screen_qs;
+        }
+        ++scanned;
+      }
+      pairs += static_cast<unsigned long long>(cnt);
+      const unsigned lm = __ballot_sync(kFull, cnt > 0);
+      if (cnt > 0) stage[__popc(lm & ((1u << lane) - 1u))] = make_int4(u, static_cast<int>(wb), k, 0);
+      __syncwarp();
+      const int n = __popc(lm);
+      for (int i = 0; i < n; i += S) {
+        int4 ed[S];
+#pragma unroll
+        for (int t = 0; t < S; ++t) ed[t] = stage[i + t < n ? i + t : i];
+        uint32_t cur[S][GV::kSlots];
+#pragma unroll
+        for (int t = 0; t < S; ++t) {
+          const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
+#pragma unroll
+          for (int r = 0; r < P; ++r) {
+            if (i + t < n && ((pmask >> r) & 1u)) {
+              load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
+            } else {
+#pragma unroll
+              for (int q = 0; q < E; ++q) cur[t][r * E + q] = 0xffffffffu;
+            }
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < S; ++t) {
+          if (i + t >= n) break;  // uniform
+          if (ed[t].z != cur_k) {  // uniform: a new vertex starts
+            if (cur_k >= 0) flush_row();
+            cur_k = ed[t].z;
+          }
+          relax_min_row<WK>(best, cur[t], static_cast<uint32_t>(ed[t].y));
+        }
+      }
+      __syncwarp();
+    }
+    if (cur_k >= 0) flush_row();
+    __syncthreads();
+    // commit: warp wib takes vertices wib, wib + 8, ...
+    for (int k = wib; k < nv; k += kWarpsPerBlock) {
+      const int32_t v = s_v[k];
+      uint32_t* row = g.values + static_cast<size_t>(v) * Qg + lane * E;
+      const uint32_t* srow = s_best + k * R + lane * E;
+      uint32_t imp = 0;
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        if (!((pmask >> r) & 1u)) continue;
+        uint32_t o[E], b[E], nvv[E];
+        load_vec<E>(row + 32 * E * r, o);
+        if constexpr (E == 4) {
+          const uint4 x = *reinterpret_cast<const uint4*>(srow + 32 * E * r);
+          b[0] = x.x; b[1] = x.y; b[2] = x.z; b[3] = x.w;
+        } else {
+          const uint2 x = *reinterpret_cast<const uint2*>(srow + 32 * E * r);
+          b[0] = x.x; b[1] = x.y;
+        }
+        uint32_t bits = 0;
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+          const bool up = ((smask >> (r * E + q)) & 1u) && b[q] < o[q];
+          nvv[q] = up ? b[q] : o[q];
+          bits |= static_cast<uint32_t>(up) << q;
+        }
+        if (bits) store_vec<E>(row + 32 * E * r, nvv);
+        imp |= bits << (r * E);
+      }
+      if (lane == 0) ++verts;
+      if (!__any_sync(kFull, imp != 0)) continue;
+      improved += __popc(imp);
+      uacc |= imp;
+      uint64_t words[P];
+      gather_vec_words<W>(imp, lane, words);
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        if (words[r]) {
+          const int wi = ((32 * r + lane) * E) >> 6;
+          lv.fnext[static_cast<size_t>(v) * W + wi] |= words[r];
+        }
+      }
+      const bool fresh = g.stamp[v] < lv.level + 1;  // uniform
+      __syncwarp();
+      if (fresh && lane == 0) g.stamp[v] = lv.level + 1;
+      ap.add<OT>(fresh && lane == 0, v, G, lv, lane);
+    }
+    __syncthreads();
+  }
+  ap.flush<OT>(G, lv, lane);
+  {
+    uint64_t words[P];
+    gather_vec_words<W>(uacc, lane, words);
+#pragma unroll
+    for (int r = 0; r < P; ++r)
+      if (words[r]) atomic_or64(lv.nactive + (((32 * r + lane) * E) >> 6), words[r]);
+  }
+  warp_add(improved, &g.ctl->lc.improved, lane);
+  warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);
+  warp_add(scanned, &g.ctl->lc.spull_edges, lane);
+  warp_add(verts, &g.ctl->lc.spull_vertices, lane);
+}
+
 // Gather level (vectorised), heavy vertices: CTA per 2048-edge chunk, warps
 // min-reduce their slices into shared memory, one atomicMin per slot.
 template <int W, typename OT, int WK>
@@ -1742,7 +1950,6 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->sdir != kDirPull || G.n_pheavy == 0) return;
   const LevelView lv = level_view(g);
-  WarpAppender ap;
   __shared__ uint32_t s_best[C * 32];
   __shared__ int2 s_stage[kWarpsPerBlock][32];
   __shared__ int32_t s_h;
@@ -1815,10 +2022,10 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
     }
     bool app = false;
     if (any && lane == 0) app = atomicMax(g.stamp + v, lv.level + 1) < lv.level + 1;
-    ap.add<OT>(app, v, G, lv, lane);
+    // one append per improved vertex-chunk: rare, a plain warp append
+    warp_append(app, v, app ? degree_of<OT>(G.row, v) : 0, lv.nlist, lv.ncount, lv.nedges, lane);
     __syncthreads();
   }
-  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(improved, &g.ctl->lc.improved, lane);
   warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);

@@ -108,7 +108,9 @@ typedef struct {
   int32_t dense_unroll;       /* edges per step of the dense SSSP kernel: 1 or 2; 0 = 1 */
   double sssp_pull_edge_ratio; /* SSSP levels gather (pull) when frontier edges >= ratio * E;
                                   <= 0: always scatter (push)                              */
-  int32_t reserved[2];
+  int32_t light_chunks;       /* SSSP gathers take light vertices in CTA chunks (groups of up
+                                 to 256 slots): 0 = on, -1 = one warp per vertex           */
+  int32_t reserved;
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 

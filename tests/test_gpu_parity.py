@@ -531,3 +531,19 @@ def test_sssp_gather_mixed_group(rmat_u32):
             np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source))
         else:
             np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
+
+
+@pytest.mark.parametrize("nq", [64, 128, 256])
+@pytest.mark.parametrize("heavy", [0, 16, 1 << 20])
+def test_sssp_gather_light_chunks(rmat_u32, nq, heavy):
+    """Light vertices gathered in CTA chunks (up to 32 vertices / 2048 in-edges,
+    a larger vertex alone; with heavy_degree 2^20 every vertex is light) give
+    the same distances as one warp per vertex and as the oracle."""
+    g, graph = rmat_u32
+    src = g.pick_sources(nq, seed=131)
+    ref, _ = oracle.batch("sssp", g, src)
+    descs = [cgp.QueryDescriptor(int(s), "sssp") for s in src]
+    for chunks in (True, False):
+        r = cgp.run_batch(graph, descs, cgp.RunOptions(traversal_mode="pull", heavy_degree=heavy,
+                                                       light_chunks=chunks), layout="query")
+        np.testing.assert_array_equal(r.values, ref)
