@@ -187,7 +187,7 @@ CLASS_KERNELS = {
     "bfs_push": "k_bfs_push, k_bfs_push_heavy",
     "bfs_pull": "k_bfs_pull, k_bfs_pull_heavy(_commit)",
     "sssp_scatter": "k_sssp_push, k_sssp_dense, k_sssp_push_heavy",
-    "sssp_gather": "k_sssp_pull_vec, k_sssp_pull_heavy_vec",
+    "sssp_gather": "k_sssp_pull_chunked, k_sssp_pull_heavy_vec",
 }
 
 
@@ -511,10 +511,15 @@ def main():
     if dom:
         k = kclass[dom]
         achieved = k["bytes"] / (k["ms"] / 1e3) / 1e9
+        tr = ncu_traffic(workload_name(args), dom)
         roofline = {"bound": "hbm", "kernel": f"{dom} levels ({CLASS_KERNELS[dom]})",
                     "achieved": achieved, "peak": peak,
                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
                     "traffic": ncu_traffic(workload_name(args), dom),
+                    "traffic_note": "DRAM bytes per level (ncu); the algorithmic count charges "
+                                    "every (edge, slot) row read, L2 hits included",
+                    "dram_frac": (tr / (k["ms"] / max(1, k["launches"]) / 1e3) / 1e9 / peak
+                                  if tr else None),
                     "per": "level", "bytes_per_launch": k["bytes"] / max(1, k["launches"]),
                     "ms_per_launch": k["ms"] / max(1, k["launches"]),
                     "classes": {n: {"ms": v["ms"], "launches": v["launches"],
