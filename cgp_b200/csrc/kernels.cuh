@@ -818,6 +818,29 @@ __device__ __forceinline__ bool sssp_relax(const GroupDev& g, const LevelView& l
   return atomicMax(g.stamp + n, lv.level + 1) < lv.level + 1;
 }
 
+// Second half of sssp_relax, for callers that loaded the destination value
+// themselves (cand < the value they read): the atomicMin and its frontier,
+// union and stamp updates.  True when n must be appended.
+template <int W>
+__device__ __forceinline__ bool sssp_commit(const GroupDev& g, const LevelView& lv, int32_t n,
+                                            int q, uint32_t cand, uint64_t (&uni)[W],
+                                            unsigned long long& improved) {
+  uint32_t* dst = g.values + static_cast<size_t>(n) * static_cast<size_t>(g.Qg) + q;
+  const uint32_t old = atomicMin(dst, cand);
+  if (cand >= old) return false;
+  const uint64_t bit = 1ULL << (q & 63);
+  uint64_t* fw = lv.fnext + static_cast<size_t>(n) * W + (q >> 6);
+  if (!(*fw & bit)) atomic_or64(fw, bit);
+  uni[q >> 6] |= bit;
+  ++improved;
+  if (g.stamp[n] >= lv.level + 1) return false;
+  return atomicMax(g.stamp + n, lv.level + 1) < lv.level + 1;
+}
+
+// Pairs handled per lane per step by the sparse scatter loops: their column,
+// source and destination loads are independent and issued together.
+constexpr int kPairSteps = 4;
+
 // Relaxation with the weight already loaded (raw 32-bit pattern).
 template <int WK>
 __device__ __forceinline__ uint32_t relax_w(uint32_t du, uint32_t wbits) {
@@ -1040,28 +1063,43 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
 #pragma unroll
     for (int i = 0; i < W; ++i) s_b[wib][lane][i] = b[i];
     __syncwarp();
-    for (long long b0 = 0; b0 < total; b0 += 32) {
-      const long long p = b0 + lane;
-      int32_t nb = 0;
-      bool app = false;
-      if (p < total) {
-        int lo = 0, hi = 31;
-        while (lo < hi) {
-          int mid = (lo + hi) >> 1;
-          if (s_inc[wib][mid] > p) hi = mid;
-          else lo = mid + 1;
+    const size_t Qg = static_cast<size_t>(g.Qg);
+    for (long long b0 = 0; b0 < total; b0 += 32 * kPairSteps) {
+      int32_t nb[kPairSteps];
+      int qq[kPairSteps];
+      uint32_t cand[kPairSteps], cur[kPairSteps];
+#pragma unroll
+      for (int t = 0; t < kPairSteps; ++t) {
+        const long long p = b0 + 32 * t + lane;
+        nb[t] = 0;
+        qq[t] = 0;
+        cand[t] = 0xffffffffu;
+        if (p < total) {
+          int lo = 0, hi = 31;
+          while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (s_inc[wib][mid] > p) hi = mid;
+            else lo = mid + 1;
+          }
+          const long long start = lo ? s_inc[wib][lo - 1] : 0;
+          const int local = static_cast<int>(p - start);  // < kDenseBits * heavy_degree
+          const int ko = s_k[wib][lo];
+          const int eoff = local / ko;
+          const int j = local - eoff * ko;
+          qq[t] = jth_set_bit<W>(s_b[wib][lo], j);
+          const int64_t e = s_beg[wib][lo] + eoff;
+          nb[t] = G.col[e];
+          cand[t] = relax<WK>(g.values[static_cast<size_t>(s_u[wib][lo]) * Qg + qq[t]], G.w, e);
         }
-        const long long start = lo ? s_inc[wib][lo - 1] : 0;
-        const int local = static_cast<int>(p - start);  // < kDenseBits * heavy_degree
-        const int ko = s_k[wib][lo];
-        const int eoff = local / ko;
-        const int j = local - eoff * ko;
-        const int q = jth_set_bit<W>(s_b[wib][lo], j);
-        const int64_t e = s_beg[wib][lo] + eoff;
-        nb = G.col[e];
-        app = sssp_relax<W, WK>(g, lv, s_u[wib][lo], nb, q, G.w, e, uni, improved);
       }
-      ap.add<OT>(app, nb, G, lv, lane);
+#pragma unroll
+      for (int t = 0; t < kPairSteps; ++t)
+        cur[t] = cand[t] != 0xffffffffu ? g.values[static_cast<size_t>(nb[t]) * Qg + qq[t]] : 0u;
+#pragma unroll
+      for (int t = 0; t < kPairSteps; ++t) {
+        const bool app = cand[t] < cur[t] && sssp_commit<W>(g, lv, nb[t], qq[t], cand[t], uni, improved);
+        ap.add<OT>(app, nb[t], G, lv, lane);
+      }
     }
     __syncwarp();
   }
@@ -1150,18 +1188,33 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
       atomicAdd(&g.ctl->lc.sssp_pairs, static_cast<unsigned long long>(pairs));
       if (c == g.hq_start[h]) atomicAdd(&g.ctl->lc.sssp_active, static_cast<unsigned long long>(k));
     }
-    for (long long p0 = threadIdx.x & ~31; p0 < pairs; p0 += blockDim.x) {
-      const long long p = p0 + lane;
-      int32_t nb = 0;
-      bool app = false;
-      if (p < pairs) {
-        const int eoff = static_cast<int>(p) / k;  // pairs <= kHeavyChunk * kDenseBits
-        const int q = s_q[static_cast<int>(p) - eoff * k];
-        const int64_t e = cb + eoff;
-        nb = G.col[e];
-        app = sssp_relax<W, WK>(g, lv, u, nb, q, G.w, e, uni, improved);
+    const size_t Qg = static_cast<size_t>(g.Qg);
+    for (long long p0 = threadIdx.x & ~31; p0 < pairs; p0 += kPairSteps * blockDim.x) {
+      int32_t nb[kPairSteps];
+      int qq[kPairSteps];
+      uint32_t cand[kPairSteps], cur[kPairSteps];
+#pragma unroll
+      for (int t = 0; t < kPairSteps; ++t) {
+        const long long p = p0 + t * blockDim.x + lane;
+        nb[t] = 0;
+        qq[t] = 0;
+        cand[t] = 0xffffffffu;
+        if (p < pairs) {
+          const int eoff = static_cast<int>(p) / k;  // pairs <= kHeavyChunk * kDenseBits
+          qq[t] = s_q[static_cast<int>(p) - eoff * k];
+          const int64_t e = cb + eoff;
+          nb[t] = G.col[e];
+          cand[t] = relax<WK>(g.values[static_cast<size_t>(u) * Qg + qq[t]], G.w, e);
+        }
       }
-      ap.add<OT>(app, nb, G, lv, lane);
+#pragma unroll
+      for (int t = 0; t < kPairSteps; ++t)
+        cur[t] = cand[t] != 0xffffffffu ? g.values[static_cast<size_t>(nb[t]) * Qg + qq[t]] : 0u;
+#pragma unroll
+      for (int t = 0; t < kPairSteps; ++t) {
+        const bool app = cand[t] < cur[t] && sssp_commit<W>(g, lv, nb[t], qq[t], cand[t], uni, improved);
+        ap.add<OT>(app, nb[t], G, lv, lane);
+      }
     }
     __syncthreads();
   }

@@ -504,7 +504,7 @@ def test_large_mixed_batch_split_by_kind(rmat_u32, layout, order):
 @pytest.mark.parametrize("opts", [dict(traversal_mode="pull"),
                                   dict(sssp_pull_edge_ratio=0.05, heavy_degree=32)])
 def test_sssp_gather_weight_ranges(wrange, opts):
-    """256-slot vector gathers with small, medium, large and near-overflow
+    """256-slot gathers and scatters with small, medium, large and near-overflow
     integer weights (sums saturate at UINT32_MAX exactly like the oracle's)."""
     g = cgp.gen_rmat(12, 8, seed=121).with_weights("u32", wrange[0], wrange[1], seed=122)
     graph = cgp.CsrGraph(g)
