@@ -511,7 +511,7 @@ def test_sssp_gather_weight_ranges(wrange, opts):
     src = g.pick_sources(256, seed=123)
     ref, _ = oracle.batch("sssp", g, src)
     r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
-                      cgp.RunOptions(**opts), layout="query")
+                      cgp.RunOptions(mask_words=4, **opts), layout="query")
     assert r.mask_words == 4
     np.testing.assert_array_equal(r.values, ref)
 
@@ -524,7 +524,8 @@ def test_sssp_gather_mixed_group(rmat_u32):
     descs = [cgp.QueryDescriptor(int(s), "bfs" if i % 8 == 0 else "sssp")
              for i, s in enumerate(src)]
     r = cgp.run_heterogeneous(graph, cgp.HybridQueryBatch(descs),
-                              options=cgp.RunOptions(traversal_mode="pull"), layout="query")
+                              options=cgp.RunOptions(traversal_mode="pull", mask_words=4),
+                              layout="query")
     assert r.groups == 1
     for i, d in enumerate(descs):
         if d.kind == "bfs":
@@ -545,5 +546,7 @@ def test_sssp_gather_light_chunks(rmat_u32, nq, heavy):
     descs = [cgp.QueryDescriptor(int(s), "sssp") for s in src]
     for chunks in (True, False):
         r = cgp.run_batch(graph, descs, cgp.RunOptions(traversal_mode="pull", heavy_degree=heavy,
-                                                       light_chunks=chunks), layout="query")
+                                                       light_chunks=chunks, mask_words=nq // 64),
+                          layout="query")
         np.testing.assert_array_equal(r.values, ref)
+
