@@ -170,13 +170,23 @@ void build_heavy(const std::vector<int64_t>& row, int64_t V, int64_t h, HeavyTab
 }
 
 void build_light_chunks(const std::vector<int64_t>& row, int64_t V, int64_t h, LightChunks& t) {
+  // light vertices by in-degree, largest first (ties by id): CTAs take chunks
+  // roughly in this order, so within a gather level the better-connected
+  // vertices settle first and the rest read their lowered distances
+  std::vector<int32_t> order;
+  for (int64_t v = 0; v < V; ++v) {
+    const int64_t d = row[v + 1] - row[v];
+    if (d > 0 && d <= h) order.push_back(static_cast<int32_t>(v));
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+    return row[a + 1] - row[a] > row[b + 1] - row[b];
+  });
   std::vector<int32_t> vs;
   std::vector<int32_t> cs{0};
   int cur_v = 0;
   int64_t cur_e = 0;
-  for (int64_t v = 0; v < V; ++v) {
+  for (const int32_t v : order) {
     const int64_t d = row[v + 1] - row[v];
-    if (d == 0 || d > h) continue;
     if (cur_v > 0 && (cur_v == dev::kLightChunkVerts || cur_e + d > dev::kLightChunkEdges)) {
       cs.push_back(static_cast<int32_t>(vs.size()));
       cur_v = 0;
@@ -377,6 +387,15 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
     }
     if (L.spull) {
       if (kt) kt->mark(kClassSsspPull, s);
+      // heavy vertices first: the light vertices' gathers of the same level
+      // then read the hubs' lowered distances (the level is Gauss-Seidel)
+      if (L.G.n_pheavy) {
+        if (L.gvec)
+          k_sssp_pull_heavy_vec<W, OT, WK><<<L.gr.gather_heavy_vec, kBlock, 0, s>>>(L.g, L.G);
+        else
+          k_sssp_pull_heavy<W, OT, WK><<<L.gr.gather_heavy, kBlock, 0, s>>>(L.g, L.G);
+        ++n;
+      }
       if constexpr (W <= 4) {
         if (L.gvec && L.lchunks) {
           k_sssp_pull_chunked<W, OT, WK><<<L.gr.gather_chunked, kBlock, 0, s>>>(L.g, L.G);
@@ -390,14 +409,8 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
       else
         k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
       ++n;
-      if (L.G.n_pheavy) {
-        if (L.gvec)
-          k_sssp_pull_heavy_vec<W, OT, WK><<<L.gr.gather_heavy_vec, kBlock, 0, s>>>(L.g, L.G);
-        else
-          k_sssp_pull_heavy<W, OT, WK><<<L.gr.gather_heavy, kBlock, 0, s>>>(L.g, L.G);
-        ++n;
-      }
     }
+
   }
   if (kt) kt->mark(kClassLevelEnd, s);
   k_level_end<W><<<1, 32, 0, s>>>(L.g);

@@ -50,11 +50,12 @@ struct HeavyTable {
 };
 
 // Heavy tables of the traversal CSR and of the pull CSR for one threshold.
-// Chunks of light vertices of the pull CSR (in-degree in [1, threshold]):
-// runs of consecutive such vertices with at most kLightChunkVerts vertices
-// and kLightChunkEdges in-edges (a single larger vertex forms its own chunk).
+// Chunks of light vertices of the pull CSR (in-degree in [1, threshold]),
+// taken in order of decreasing in-degree: runs with at most kLightChunkVerts
+// vertices and kLightChunkEdges in-edges (a single larger vertex forms its own
+// chunk).
 struct LightChunks {
-  DevBuf vertices;     // int32 [n] light vertices in id order
+  DevBuf vertices;     // int32 [n] light vertices, largest in-degree first
   DevBuf chunk_start;  // int32 [chunks + 1] positions in `vertices`
   int32_t n = 0;
   int32_t chunks = 0;
