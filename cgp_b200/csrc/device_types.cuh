@@ -88,6 +88,7 @@ struct LevelCtl {
   unsigned long long sssp_pull_edge_threshold;  // gather when frontier edges reach it
   unsigned long long dense_count;  // SSSP vertices queued for the dense kernel this level
   unsigned long long hq_packed;    // heavy frontier queue: count << 40 | chunks, this level
+  unsigned long long prev_improved; // SSSP entries improved by the previous level
   LevelCounters lc;                // counters of the current level
   LevelCounters total;             // sums over all levels
 };

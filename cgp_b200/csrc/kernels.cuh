@@ -1570,27 +1570,43 @@ __device__ __forceinline__ void gather_vec_words(uint32_t bits, int lane,
 }
 
 // Whether the gather screens in-edges by their source's frontier mask: -1
-// when the frontier's out-edges are less than half of all edges; otherwise
-// the number of SSSP slots (every source is then read, which skips a
-// dependent mask load per 32 in-edges and costs little: almost every edge's
-// source is live).
+// when the frontier's out-edges are less than half of all edges, or when its
+// (vertex, slot) entries are sparse (the previous level improved fewer than
+// 1/32 of the frontier's vertices x SSSP slots); screened gathers skip sources
+// with no frontier bit and, within a source, the 32-slot chunks with none.
+// Otherwise the number of SSSP slots: every source row is read whole, which
+// skips a dependent mask load per 32 in-edges and costs little when almost
+// every (source, slot) is live.
 template <int W>
 __device__ __forceinline__ int gather_screen_qs(const LevelCtl* ctl, const LevelView& lv,
                                                 int64_t E) {
-  if (2 * ctl->edges[lv.par] < static_cast<unsigned long long>(E)) return -1;
   int qs = 0;
 #pragma unroll
   for (int i = 0; i < W; ++i) qs += __popcll(ctl->sssp_bits[i]);
+  if (2 * ctl->edges[lv.par] < static_cast<unsigned long long>(E)) return -1;
+  if (32 * ctl->prev_improved < ctl->count[lv.par] * static_cast<unsigned long long>(qs)) return -1;
   return qs;
+}
+
+// Bit c: 32-slot chunk c of the mask has a bit set.
+template <int W>
+__device__ __forceinline__ uint32_t chunk_bits(const uint64_t (&m)[W]) {
+  uint32_t c = 0;
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    c |= (static_cast<uint32_t>(m[i]) != 0u ? 1u : 0u) << (2 * i);
+    c |= (static_cast<uint32_t>(m[i] >> 32) != 0u ? 1u : 0u) << (2 * i + 1);
+  }
+  return c;
 }
 
 // Gathers in-edges [eb, ee) into best[] (vector layout).  `stage` is this
 // warp's 32-entry shared staging array.  All lanes call.
-template <int W, int WK>
+template <int W, int WK, bool kChunks = true>
 __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGraph& G,
                                                  const LevelView& lv, const uint64_t* sb,
                                                  uint32_t pmask, int64_t eb, int64_t ee,
-                                                 int lane, int2* stage,
+                                                 int lane, int4* stage,
                                                  uint32_t (&best)[GatherVec<W>::kSlots],
                                                  unsigned long long& pairs,
                                                  unsigned& scanned, int screen_qs) {
@@ -1605,15 +1621,21 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
     int k = 0;
     int32_t u = 0;
     uint32_t wb = 0;
+    uint32_t cm = 0xffffffffu;  // 32-slot chunks of the source to read
     if (e < ee) {
       u = G.pcol[e];
       wb = weight_bits<WK>(G.pw, e);
       if (screen_qs < 0) {
-        // sparse frontier: skip in-edges whose source has no SSSP frontier bit
+        // sparse frontier: skip in-edges whose source has no SSSP frontier
+        // bit, and the source's 32-slot chunks that have none
         uint64_t m[W];
         load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
 #pragma unroll
-        for (int i = 0; i < W; ++i) k += __popcll(m[i] & sb[i]);
+        for (int i = 0; i < W; ++i) {
+          m[i] &= sb[i];
+          k += __popcll(m[i]);
+        }
+        if constexpr (kChunks) cm = chunk_bits<W>(m);
       } else {
         k = screen_qs;  // dense frontier: every in-edge is gathered (no mask load)
       }
@@ -1621,12 +1643,14 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
     }
     pairs += static_cast<unsigned long long>(k);
     const unsigned lm = __ballot_sync(kFull, k > 0);
-    if (k > 0) stage[__popc(lm & ((1u << lane) - 1u))] = make_int2(u, static_cast<int>(wb));
+    if (k > 0)
+      stage[__popc(lm & ((1u << lane) - 1u))] =
+          make_int4(u, static_cast<int>(wb), 0, kChunks ? static_cast<int>(cm) : -1);
     __syncwarp();
     const int n = __popc(lm);
     int i = 0;
     for (; i + S <= n; i += S) {
-      int2 ed[S];
+      int4 ed[S];
 #pragma unroll
       for (int t = 0; t < S; ++t) ed[t] = stage[i + t];
       uint32_t cur[S][GV::kSlots];
@@ -1635,7 +1659,7 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
         const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
 #pragma unroll
         for (int r = 0; r < P; ++r) {
-          if ((pmask >> r) & 1u) {
+          if (((pmask >> r) & 1u) && (!kChunks || ((ed[t].w >> (((32 * r + lane) * E) >> 5)) & 1))) {
             load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
           } else {
 #pragma unroll
@@ -1649,7 +1673,7 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
     if (i < n) {
       // the remaining 1..S-1 edges in one step (uniform predicates), so that
       // a short list costs one round trip instead of one per edge
-      int2 ed[S];
+      int4 ed[S];
 #pragma unroll
       for (int t = 0; t < S; ++t) ed[t] = stage[i + t < n ? i + t : i];
       uint32_t cur[S][GV::kSlots];
@@ -1658,7 +1682,7 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
         const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
 #pragma unroll
         for (int r = 0; r < P; ++r) {
-          if (i + t < n && ((pmask >> r) & 1u)) {
+          if (i + t < n && ((pmask >> r) & 1u) && (!kChunks || ((ed[t].w >> (((32 * r + lane) * E) >> 5)) & 1))) {
             load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
           } else {
 #pragma unroll
@@ -1682,7 +1706,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   constexpr int P = GV::kParts;
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->sdir != kDirPull) return;
-  __shared__ int2 s_stage[kWarpsPerBlock][32];
+  __shared__ int4 s_stage[kWarpsPerBlock][32];
   const LevelView lv = level_view(g);
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -1873,6 +1897,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
       int cnt = 0, k = 0;
       int32_t u = 0;
       uint32_t wb = 0;
+      uint32_t cm = 0xffffffffu;  // 32-slot chunks of the source to read
       if (f < fb) {
         int lo = 0, hi = nv - 1;  // owner: last k with s_pre[k] <= f
         while (lo < hi) {
@@ -1888,7 +1913,11 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
           uint64_t m[W];
           load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
 #pragma unroll
-          for (int i = 0; i < W; ++i) cnt += __popcll(m[i] & sb[i]);
+          for (int i = 0; i < W; ++i) {
+            m[i] &= sb[i];
+            cnt += __popcll(m[i]);
+          }
+          cm = chunk_bits<W>(m);
         } else {
           cnt = screen_qs;
         }
@@ -1896,7 +1925,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
       }
       pairs += static_cast<unsigned long long>(cnt);
       const unsigned lm = __ballot_sync(kFull, cnt > 0);
-      if (cnt > 0) stage[__popc(lm & ((1u << lane) - 1u))] = make_int4(u, static_cast<int>(wb), k, 0);
+      if (cnt > 0)
+        stage[__popc(lm & ((1u << lane) - 1u))] = make_int4(u, static_cast<int>(wb), k, static_cast<int>(cm));
       __syncwarp();
       const int n = __popc(lm);
       for (int i = 0; i < n; i += S) {
@@ -1909,7 +1939,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
           const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
 #pragma unroll
           for (int r = 0; r < P; ++r) {
-            if (i + t < n && ((pmask >> r) & 1u)) {
+            if (i + t < n && ((pmask >> r) & 1u) && ((ed[t].w >> (((32 * r + lane) * E) >> 5)) & 1)) {
               load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
             } else {
 #pragma unroll
@@ -2004,7 +2034,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   if (ctl->done || ctl->sdir != kDirPull || G.n_pheavy == 0) return;
   const LevelView lv = level_view(g);
   __shared__ uint32_t s_best[C * 32];
-  __shared__ int2 s_stage[kWarpsPerBlock][32];
+  __shared__ int4 s_stage[kWarpsPerBlock][32];
   __shared__ int32_t s_h;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -2044,8 +2074,10 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
     uint32_t best[GV::kSlots];
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) best[j] = 0xffffffffu;
-    gather_edges_vec<W, WK>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best, pairs, scanned,
-                            screen_qs);
+    // heavy vertices read whole source rows (chunk skipping costs this kernel
+    // more registers than it saves on its long in-edge lists)
+    gather_edges_vec<W, WK, false>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best, pairs,
+                                   scanned, screen_qs);
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) {
       const int q = (32 * (j / E) + lane) * E + (j % E);
@@ -2159,6 +2191,7 @@ __global__ void k_level_end(GroupDev g) {
   ctl->total.sssp_pairs += ctl->lc.sssp_pairs;
   ctl->total.sssp_active += ctl->lc.sssp_active;
   ctl->total.improved += ctl->lc.improved;
+  ctl->prev_improved = ctl->lc.improved;
   ctl->total.spull_vertices += ctl->lc.spull_vertices;
   ctl->total.spull_edges += ctl->lc.spull_edges;
   ctl->lc = LevelCounters{};
