@@ -313,6 +313,7 @@ struct Grids {
   int gather_vec;
   int gather_heavy_vec;
   int gather_chunked;
+  int gather_heavy_vec2;
 };
 
 struct LevelLaunch {
@@ -390,10 +391,17 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
       // heavy vertices first: the light vertices' gathers of the same level
       // then read the hubs' lowered distances (the level is Gauss-Seidel)
       if (L.G.n_pheavy) {
-        if (L.gvec)
-          k_sssp_pull_heavy_vec<W, OT, WK><<<L.gr.gather_heavy_vec, kBlock, 0, s>>>(L.g, L.G);
-        else
+        if (L.gvec && W <= 4) {
+          // whole-row and chunk-skipping variants; each returns at once on the
+          // other's levels
+          k_sssp_pull_heavy_vec<W, OT, WK, 1><<<L.gr.gather_heavy_vec, kBlock, 0, s>>>(L.g, L.G);
+          k_sssp_pull_heavy_vec<W, OT, WK, 2><<<L.gr.gather_heavy_vec2, kBlock, 0, s>>>(L.g, L.G);
+          ++n;
+        } else if (L.gvec) {
+          k_sssp_pull_heavy_vec<W, OT, WK, 0><<<L.gr.gather_heavy_vec, kBlock, 0, s>>>(L.g, L.G);
+        } else {
           k_sssp_pull_heavy<W, OT, WK><<<L.gr.gather_heavy, kBlock, 0, s>>>(L.g, L.G);
+        }
         ++n;
       }
       if constexpr (W <= 4) {
@@ -422,11 +430,12 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
 template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
   static int tile = 0, heavy = 0, dense = 0, dense2 = 0, gather = 0, gather_heavy = 0;
-  static int gather_vec = 0, gather_heavy_vec = 0, gather_chunked = 0;
+  static int gather_vec = 0, gather_heavy_vec = 0, gather_chunked = 0, gather_heavy_vec2 = 0;
   if (tile == 0) {
     if constexpr (W <= 4) gather_chunked = occupancy_grid(k_sssp_pull_chunked<W, OT, WK>, sms);
     gather_vec = occupancy_grid(k_sssp_pull_vec<W, OT, WK>, sms);
-    gather_heavy_vec = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK>, sms);
+    gather_heavy_vec = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK, (W <= 4 ? 1 : 0)>, sms);
+    gather_heavy_vec2 = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK, 2>, sms);
     gather = occupancy_grid(k_sssp_pull<W, OT, WK>, sms);
     gather_heavy = occupancy_grid(k_sssp_pull_heavy<W, OT, WK>, sms);
     dense = occupancy_grid(k_sssp_dense<W, OT, WK, 1>, sms);
@@ -449,6 +458,7 @@ Grids grids_t(int sms) {
   g.gather_vec = gather_vec;
   g.gather_heavy_vec = gather_heavy_vec;
   g.gather_chunked = gather_chunked;
+  g.gather_heavy_vec2 = gather_heavy_vec2;
   return g;
 }
 

@@ -1573,7 +1573,7 @@ __device__ __forceinline__ void gather_vec_words(uint32_t bits, int lane,
 // when the frontier's out-edges are less than half of all edges, or when its
 // (vertex, slot) entries are sparse (the previous level improved fewer than
 // 1/32 of the frontier's vertices x SSSP slots); screened gathers skip sources
-// with no frontier bit and, within a source, the 32-slot chunks with none.
+// with no frontier bit and, within a source row, the 32-slot chunks with none.
 // Otherwise the number of SSSP slots: every source row is read whole, which
 // skips a dependent mask load per 32 in-edges and costs little when almost
 // every (source, slot) is live.
@@ -1600,6 +1600,14 @@ __device__ __forceinline__ uint32_t chunk_bits(const uint64_t (&m)[W]) {
   return c;
 }
 
+// Whether the lane reads part r of a source row whose 32-slot chunk bits are
+// `cm`.
+template <int W>
+__device__ __forceinline__ bool chunk_live(uint32_t cm, int r, int lane) {
+  constexpr int E = GatherVec<W>::kElem;
+  return (cm >> (((32 * r + lane) * E) >> 5)) & 1u;
+}
+
 // Gathers in-edges [eb, ee) into best[] (vector layout).  `stage` is this
 // warp's 32-entry shared staging array.  All lanes call.
 template <int W, int WK, bool kChunks = true>
@@ -1621,13 +1629,13 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
     int k = 0;
     int32_t u = 0;
     uint32_t wb = 0;
-    uint32_t cm = 0xffffffffu;  // 32-slot chunks of the source to read
+    uint32_t cm = 0xffffffffu;  // 32-slot chunks of the source row to read
     if (e < ee) {
       u = G.pcol[e];
       wb = weight_bits<WK>(G.pw, e);
       if (screen_qs < 0) {
         // sparse frontier: skip in-edges whose source has no SSSP frontier
-        // bit, and the source's 32-slot chunks that have none
+        // bit, and the source row's 32-slot chunks that have none
         uint64_t m[W];
         load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
 #pragma unroll
@@ -1659,7 +1667,7 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
         const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
 #pragma unroll
         for (int r = 0; r < P; ++r) {
-          if (((pmask >> r) & 1u) && (!kChunks || ((ed[t].w >> (((32 * r + lane) * E) >> 5)) & 1))) {
+          if (((pmask >> r) & 1u) && (!kChunks || chunk_live<W>(static_cast<uint32_t>(ed[t].w), r, lane))) {
             load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
           } else {
 #pragma unroll
@@ -1682,7 +1690,7 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
         const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
 #pragma unroll
         for (int r = 0; r < P; ++r) {
-          if (i + t < n && ((pmask >> r) & 1u) && (!kChunks || ((ed[t].w >> (((32 * r + lane) * E) >> 5)) & 1))) {
+          if (i + t < n && ((pmask >> r) & 1u) && (!kChunks || chunk_live<W>(static_cast<uint32_t>(ed[t].w), r, lane))) {
             load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
           } else {
 #pragma unroll
@@ -1897,7 +1905,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
       int cnt = 0, k = 0;
       int32_t u = 0;
       uint32_t wb = 0;
-      uint32_t cm = 0xffffffffu;  // 32-slot chunks of the source to read
+      uint32_t cm = 0xffffffffu;  // 32-slot chunks of the source row to read
       if (f < fb) {
         int lo = 0, hi = nv - 1;  // owner: last k with s_pre[k] <= f
         while (lo < hi) {
@@ -1939,7 +1947,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
           const uint32_t* row = lanebase + static_cast<size_t>(ed[t].x) * Qg;
 #pragma unroll
           for (int r = 0; r < P; ++r) {
-            if (i + t < n && ((pmask >> r) & 1u) && ((ed[t].w >> (((32 * r + lane) * E) >> 5)) & 1)) {
+            if (i + t < n && ((pmask >> r) & 1u) && chunk_live<W>(static_cast<uint32_t>(ed[t].w), r, lane)) {
               load_vec_cg<E>(row + 32 * E * r, &cur[t][r * E]);
             } else {
 #pragma unroll
@@ -2025,7 +2033,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
 
 // Gather level (vectorised), heavy vertices: CTA per 2048-edge chunk, warps
 // min-reduce their slices into shared memory, one atomicMin per slot.
-template <int W, typename OT, int WK>
+// kMode 0: every gather level, whole source rows; 1: only levels that read
+// whole rows (dense entries); 2: only screened levels (sparse entries), with
+// the source rows' 32-slot chunks without frontier bits skipped.  Modes 1 and 2
+// are launched together (groups of <= 256 slots) so that each level runs the
+// variant whose register budget suits it.
+template <int W, typename OT, int WK, int kMode>
 __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevGraph G) {
   using GV = GatherVec<W>;
   constexpr int E = GV::kElem;
@@ -2043,6 +2056,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
   const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  if ((kMode == 1 && screen_qs < 0) || (kMode == 2 && screen_qs >= 0)) return;
   const size_t Qg = static_cast<size_t>(g.Qg);
   uint64_t uni[W];
 #pragma unroll
@@ -2074,10 +2088,8 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
     uint32_t best[GV::kSlots];
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) best[j] = 0xffffffffu;
-    // heavy vertices read whole source rows (chunk skipping costs this kernel
-    // more registers than it saves on its long in-edge lists)
-    gather_edges_vec<W, WK, false>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best, pairs,
-                                   scanned, screen_qs);
+    gather_edges_vec<W, WK, kMode == 2>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best,
+                                        pairs, scanned, screen_qs);
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) {
       const int q = (32 * (j / E) + lane) * E + (j % E);
