@@ -40,6 +40,11 @@ __device__ __forceinline__ void load_mask(const uint64_t* p, uint64_t (&m)[W]) {
   }
 }
 
+// Asks L2 to fetch the line holding p (no register is written, nothing waits).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <int W>
 __device__ __forceinline__ void store_mask(uint64_t* p, const uint64_t (&m)[W]) {
   if constexpr (W % 2 == 0) {
@@ -1638,6 +1643,8 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
         // bit, and the source row's 32-slot chunks that have none
         uint64_t m[W];
         load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
+        // the next batch's source masks move to L2 while this batch's rows load
+        if (e + 32 < ee) prefetch_l2(lv.fcur + static_cast<size_t>(G.pcol[e + 32]) * W);
 #pragma unroll
         for (int i = 0; i < W; ++i) {
           m[i] &= sb[i];
@@ -1920,6 +1927,17 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
         if (screen_qs < 0) {
           uint64_t m[W];
           load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
+          // the next batch's source masks move to L2 while this batch's rows load
+          const int fn = f + 32;
+          if (fn < fb) {
+            int a = k, b = nv - 1;  // owner of fn: last k' >= k with s_pre[k'] <= fn
+            while (a < b) {
+              const int mid = (a + b + 1) >> 1;
+              if (s_pre[mid] <= fn) a = mid;
+              else b = mid - 1;
+            }
+            prefetch_l2(lv.fcur + static_cast<size_t>(G.pcol[s_beg[a] + (fn - s_pre[a])]) * W);
+          }
 #pragma unroll
           for (int i = 0; i < W; ++i) {
             m[i] &= sb[i];
