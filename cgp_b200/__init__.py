@@ -8,14 +8,15 @@ from ._native import (BFS_UNREACHED, U32_UNREACHED, CgpError, CgpInvalidArgument
                       CgpOutOfMemory, declared_symbols, lib)
 from .api import (CsrGraph, Enactor, HostCsr, HybridQueryBatch, IterationProfile,  # noqa: F401
                   QueryBatch, QueryDescriptor, RunOptions, RunResult, csr_from_edges,
-                  gen_chung_lu, gen_grid, gen_rmat, load_binary_csr, load_matrix_market, run,
-                  run_batch, run_heterogeneous, set_device,
+                  gen_chung_lu, gen_grid, gen_rmat, load_binary_csr, load_galois_gr,
+                  load_matrix_market, run, run_batch, run_heterogeneous, set_device,
                   Server, RequestInfo, run_replenish_pipeline, autotune)
 
 __all__ = [
     "CsrGraph", "Enactor", "HostCsr", "HybridQueryBatch", "IterationProfile", "QueryBatch",
     "QueryDescriptor", "RunOptions", "RunResult", "csr_from_edges", "gen_chung_lu", "gen_grid",
-    "gen_rmat", "load_binary_csr", "load_matrix_market", "run", "run_batch",
-    "run_heterogeneous", "set_device", "Server", "RequestInfo", "run_replenish_pipeline", "autotune", "BFS_UNREACHED", "U32_UNREACHED", "CgpError", "CgpInvalidArgument",
+    "gen_rmat", "load_binary_csr", "load_galois_gr", "load_matrix_market", "run", "run_batch",
+    "run_heterogeneous", "set_device", "Server", "RequestInfo", "run_replenish_pipeline",
+    "autotune", "BFS_UNREACHED", "U32_UNREACHED", "CgpError", "CgpInvalidArgument",
     "CgpOutOfMemory", "declared_symbols", "lib",
 ]

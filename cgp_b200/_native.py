@@ -99,6 +99,7 @@ SIGNATURES = {
     "cgp_version": (c_char_p, []),
     "cgp_set_device": (c_int32, [c_int32]),
     "cgp_last_kernel_profile": (c_int32, [POINTER(CgpKernelProfile)]),
+    "cgp_debug_fail_allocations": (c_int32, [c_int64]),
     "cgp_graph_create": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_int32, c_int64,
                                    c_int64, c_int32, POINTER(c_void_p)]),
     "cgp_graph_destroy": (c_int32, [c_void_p]),
@@ -131,6 +132,7 @@ SIGNATURES = {
                                    c_void_p]),
     "cgp_load_matrix_market": (c_int32, [c_char_p, POINTER(CgpHostCsr)]),
     "cgp_load_binary_csr": (c_int32, [c_char_p, POINTER(CgpHostCsr)]),
+    "cgp_load_galois_gr": (c_int32, [c_char_p, c_int32, POINTER(CgpHostCsr)]),
     "cgp_host_csr_free": (None, [POINTER(CgpHostCsr)]),
 }
 

@@ -153,6 +153,16 @@ def load_binary_csr(path: str) -> HostCsr:
     return _take_csr(h)
 
 
+def load_galois_gr(path: str, read_edge_data: bool = False) -> HostCsr:
+    """Galois .gr version 1 (load_gr, cgp/examples/algorithms/bfs/cgp_bfs.cu:215-260):
+    topology only like the reference, or with 4-byte edge data as uint32
+    weights when read_edge_data is set."""
+    h = N.CgpHostCsr()
+    N.check(N.lib().cgp_load_galois_gr(str(path).encode(), int(read_edge_data), ctypes.byref(h)),
+            "cgp_load_galois_gr")
+    return _take_csr(h)
+
+
 def set_device(device: int) -> None:
     """Selects the CUDA device of this thread's subsequent library calls."""
     N.check(N.lib().cgp_set_device(int(device)), "cgp_set_device")

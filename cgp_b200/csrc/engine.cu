@@ -9,6 +9,7 @@
 // one-thread kernel at the end of each level, and the host only looks at the
 // control block once per chunk of levels.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <numeric>
@@ -21,6 +22,20 @@ namespace cgp {
 using namespace dev;
 
 // ------------------------------------------------------------- buffers
+namespace {
+// Fault-injection hook for tests: >= 0 counts down the device allocations
+// still allowed before one fails as if the device were out of memory; -1 off.
+std::atomic<int64_t> g_fail_alloc_countdown{-1};
+
+bool injected_alloc_failure() {
+  int64_t c = g_fail_alloc_countdown.load();
+  while (c >= 0) {
+    if (g_fail_alloc_countdown.compare_exchange_weak(c, c - 1)) return c == 0;
+  }
+  return false;
+}
+}  // namespace
+
 DevBuf::~DevBuf() {
   if (p) cudaFree(p);
 }
@@ -31,6 +46,9 @@ bool DevBuf::ensure(size_t need) {
   p = nullptr;
   bytes = 0;
   size_t alloc = std::max<size_t>(need, 256);
+  if (injected_alloc_failure())
+    throw ApiError{CGP_ERR_OOM, "cudaMalloc of " + std::to_string(alloc) +
+                                    " bytes failed (injected by cgp_debug_fail_allocations)"};
   cudaError_t e = cudaMalloc(&p, alloc);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -548,22 +566,30 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   const HeavyPair& hp = g->heavy_for(hth);
   bool moved = false;
   const size_t mask_bytes = static_cast<size_t>(V) * W * 8;
-  moved |= ws->visited.ensure(mask_bytes);
-  moved |= ws->fbuf0.ensure(mask_bytes);
-  moved |= ws->fbuf1.ensure(mask_bytes);
-  moved |= ws->list0.ensure(static_cast<size_t>(V) * 4);
-  moved |= ws->list1.ensure(static_cast<size_t>(V) * 4);
-  moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
-  moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8);
-  moved |= ws->hq_vertex.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 4);
-  moved |= ws->hq_start.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 8);
-  if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
-  if (spec.depth_mode == kDepthPlanes) {
-    moved |= ws->planes.ensure(static_cast<size_t>(kInitialPlanes) * mask_bytes);
-  } else if (spec.external_values == nullptr) {
-    moved |= ws->values.ensure(static_cast<size_t>(V) * spec.Qg * 4);
+  try {
+    moved |= ws->visited.ensure(mask_bytes);
+    moved |= ws->fbuf0.ensure(mask_bytes);
+    moved |= ws->fbuf1.ensure(mask_bytes);
+    moved |= ws->list0.ensure(static_cast<size_t>(V) * 4);
+    moved |= ws->list1.ensure(static_cast<size_t>(V) * 4);
+    moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
+    moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8);
+    moved |= ws->hq_vertex.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 4);
+    moved |= ws->hq_start.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 8);
+    if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
+    if (spec.depth_mode == kDepthPlanes) {
+      moved |= ws->planes.ensure(static_cast<size_t>(kInitialPlanes) * mask_bytes);
+    } else if (spec.external_values == nullptr) {
+      moved |= ws->values.ensure(static_cast<size_t>(V) * spec.Qg * 4);
+    }
+    if (o.profile_iterations) moved |= ws->prof.ensure(kProfileCap * sizeof(LevelProfile));
+  } catch (...) {
+    // a failed ensure() has already freed its old block: graphs captured with
+    // the old pointers must never be replayed
+    ws->generation++;
+    ws->clear_graphs();
+    throw;
   }
-  if (o.profile_iterations) moved |= ws->prof.ensure(kProfileCap * sizeof(LevelProfile));
   if (moved) {
     ws->generation++;
     ws->clear_graphs();
@@ -996,6 +1022,11 @@ cgp_status cgp_last_profiles(cgp_level_profile* out, int32_t cap, int32_t* count
       out[i].kernel_ms = i < static_cast<int>(t_level_ms.size()) ? t_level_ms[i] : 0.0f;
     }
   }
+  return CGP_OK;
+}
+
+cgp_status cgp_debug_fail_allocations(int64_t after) {
+  g_fail_alloc_countdown.store(after < 0 ? -1 : after);
   return CGP_OK;
 }
 

@@ -147,4 +147,72 @@ cgp_status cgp_load_binary_csr(const char* dir, cgp_host_csr* out) {
   return CGP_OK;
 }
 
+// Galois binary graph, version 1 (the reader of cgp/examples/algorithms/bfs/
+// cgp_bfs.cu:215-260): four uint64 header words (version = 1, bytes of edge
+// data per edge, vertex count V, edge count E), V uint64 row ends, E uint32
+// destinations, padding to 8 bytes when E is odd, then E edge-data records.
+// The reference loader reads the topology only (unit weights); with
+// read_edge_data != 0 and 4-byte edge data the records are kept as uint32
+// weights.  Truncated files, other versions, sizes beyond int32 vertex ids,
+// decreasing row ends and destinations outside [0, V) are rejected.
+cgp_status cgp_load_galois_gr(const char* path, int32_t read_edge_data, cgp_host_csr* out) {
+  cgp::clear_error();
+  if (path == nullptr || out == nullptr) return cgp::set_error(CGP_ERR_INVALID_ARG, "NULL argument");
+  std::memset(out, 0, sizeof(*out));
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return cgp::set_error(CGP_ERR_INVALID_ARG, std::string("could not open graph: ") + path);
+  auto fail = [&](const std::string& m) {
+    std::fclose(f);
+    cgp_host_csr_free(out);
+    return cgp::set_error(CGP_ERR_INVALID_ARG, m + ": " + path);
+  };
+  uint64_t hdr[4];
+  if (std::fread(hdr, sizeof(uint64_t), 4, f) != 4) return fail("truncated .gr header");
+  const uint64_t version = hdr[0], edge_bytes = hdr[1], V64 = hdr[2], E64 = hdr[3];
+  if (version != 1) return fail("unsupported .gr version " + std::to_string(version));
+  if (V64 == 0 || V64 >= static_cast<uint64_t>(INT32_MAX))
+    return fail(".gr vertex count must be in [1, 2^31-1)");
+  if (E64 > (static_cast<uint64_t>(1) << 40)) return fail(".gr edge count too large");
+  const int64_t V = static_cast<int64_t>(V64), E = static_cast<int64_t>(E64);
+  out->num_vertices = V;
+  out->num_edges = E;
+  out->row_offsets = static_cast<int64_t*>(std::malloc(sizeof(int64_t) * (V + 1)));
+  out->col_indices = static_cast<int32_t*>(std::malloc(sizeof(int32_t) * (E > 0 ? E : 1)));
+  if (!out->row_offsets || !out->col_indices) {
+    std::fclose(f);
+    cgp_host_csr_free(out);
+    return cgp::set_error(CGP_ERR_OOM, "host allocation failed");
+  }
+  out->row_offsets[0] = 0;
+  if (std::fread(out->row_offsets + 1, sizeof(int64_t), V, f) != static_cast<size_t>(V))
+    return fail("truncated .gr row ends");
+  for (int64_t v = 0; v < V; ++v)
+    if (out->row_offsets[v + 1] < out->row_offsets[v]) return fail(".gr row ends decrease");
+  if (out->row_offsets[V] != E) return fail(".gr final row end does not match the edge count");
+  if (E > 0 && std::fread(out->col_indices, sizeof(int32_t), E, f) != static_cast<size_t>(E))
+    return fail("truncated .gr destinations");
+  for (int64_t e = 0; e < E; ++e)
+    if (out->col_indices[e] < 0 || out->col_indices[e] >= V)
+      return fail(".gr destination out of range at edge " + std::to_string(e));
+  if (read_edge_data && edge_bytes == 4 && E > 0) {
+    if (E % 2 == 1) {
+      uint32_t pad;
+      if (std::fread(&pad, 4, 1, f) != 1) return fail("truncated .gr padding");
+    }
+    out->weights = std::malloc(sizeof(uint32_t) * E);
+    if (!out->weights) {
+      std::fclose(f);
+      cgp_host_csr_free(out);
+      return cgp::set_error(CGP_ERR_OOM, "host allocation failed");
+    }
+    if (std::fread(out->weights, sizeof(uint32_t), E, f) != static_cast<size_t>(E))
+      return fail("truncated .gr edge data");
+    out->weight_kind = CGP_WEIGHT_U32;
+  } else if (read_edge_data && edge_bytes != 0 && edge_bytes != 4) {
+    return fail(".gr edge data of " + std::to_string(edge_bytes) + " bytes cannot be read as weights");
+  }
+  std::fclose(f);
+  return CGP_OK;
+}
+
 }  // extern "C"

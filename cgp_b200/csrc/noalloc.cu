@@ -20,7 +20,6 @@
 // GPU (different streams or threads on the same device) race on it, so such
 // calls must be serialised by the caller.
 #include <cstring>
-#include <mutex>
 
 #include "engine.h"
 #include "kernels.cuh"
@@ -36,26 +35,18 @@ constexpr size_t kScratchBytes = CGP_NOALLOC_SCRATCH_BYTES;
 // the device address comes from cudaGetSymbolAddress (scratch_address below).
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void* g_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on `device` (the current device),
-// looked up once per device.
-cgp_status scratch_address(int device, void** out) {
-  if (device < 0 || device >= kMaxDevices) return set_error(CGP_ERR_INVALID_ARG, "device id too large");
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (g_addr[device] == nullptr) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      cudaGetLastError();
-      return set_error(CGP_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") +
-                                         cudaGetErrorString(e));
-    }
-    g_addr[device] = p;
+// Device address of the scratch array on the current device.  Looked up on
+// every call (the lookup is cheap), so that an address cached before a
+// cudaDeviceReset or a re-created primary context is never handed to a kernel.
+cgp_status scratch_address(void** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || p == nullptr) {
+    cudaGetLastError();
+    return set_error(CGP_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") +
+                                       cudaGetErrorString(e));
   }
-  *out = g_addr[device];
+  *out = p;
   return CGP_OK;
 }
 
@@ -108,6 +99,15 @@ void run_levels(const GroupDev& g, const DevGraph& G, bool pull, int64_t V, int 
   }
 }
 
+// The status word the level kernels raise (0 = clean), read after the loop.
+uint32_t read_status(const GroupDev& g, cudaStream_t s) {
+  uint32_t st = 0;
+  ck(cudaMemcpyAsync(&st, reinterpret_cast<char*>(g.ctl) + offsetof(LevelCtl, status), sizeof(st),
+                     cudaMemcpyDeviceToHost, s), "read status");
+  ck(cudaStreamSynchronize(s), "read status");
+  return st;
+}
+
 template <int W>
 void run_w(const GroupDev& g, const DevGraph& G, bool pull, int64_t V, int nq, uint32_t* out,
            int offset_bytes, cudaStream_t s) {
@@ -144,12 +144,11 @@ extern "C" cgp_status cgp_bfs_batch_noalloc(const void* row_offsets, int32_t off
     return set_error(CGP_ERR_INVALID_ARG,
                      "graph too large for the fixed scratch array: needs " + std::to_string(need) +
                          " bytes, the maximum is " + std::to_string(kScratchBytes) +
-                         " (about 36*V + 8 KiB bytes for up to 64 queries)");
+                         " (about 17 KiB plus 36, 60 or 108 bytes per vertex for up to 64, "
+                         "128 or 256 queries)");
   try {
-    int device = 0;
-    ck(cudaGetDevice(&device), "cudaGetDevice");
     void* base = nullptr;
-    cgp_status st = scratch_address(device, &base);
+    cgp_status st = scratch_address(&base);
     if (st != CGP_OK) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int64_t V = num_vertices;
@@ -223,6 +222,9 @@ extern "C" cgp_status cgp_bfs_batch_noalloc(const void* row_offsets, int32_t off
     }
     ck(cudaGetLastError(), "noalloc launch");
     ck(cudaStreamSynchronize(s), "noalloc");
+    const uint32_t dstatus = read_status(g, s);
+    if (dstatus != 0)
+      return set_error(CGP_ERR_DEVICE, "device status " + std::to_string(dstatus));
     return CGP_OK;
   } catch (...) {
     return translate_exception();

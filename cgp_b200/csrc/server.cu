@@ -562,6 +562,10 @@ cgp_status cgp_server_create(cgp_graph* graph, int32_t slots, const cgp_options*
     return CGP_OK;
   } catch (...) {
     cgp_status st = translate_exception();
+    if (sv->stream) cudaStreamSynchronize(sv->stream);
+    if (sv->h_admit) cudaFreeHost(sv->h_admit);
+    if (sv->h_retire) cudaFreeHost(sv->h_retire);
+    if (sv->h_clear) cudaFreeHost(sv->h_clear);
     delete sv;
     return st;
   }

@@ -236,6 +236,13 @@ cgp_status cgp_batch_run(cgp_graph* g, const cgp_query* queries, int32_t nq,
 cgp_status cgp_autotune(cgp_graph* g, const cgp_query* sample, int32_t n,
                         cgp_options* opts, int32_t reps);
 
+/* Fault-injection hook for tests (no counterpart in the reference): the
+ * after-th next device allocation the library makes (0 = the very next one)
+ * fails as if cudaMalloc had run out of memory, after which the hook disarms
+ * itself; after < 0 disarms it.  The failing call returns CGP_ERR_OOM and
+ * leaves the graph and its cached state usable. */
+cgp_status cgp_debug_fail_allocations(int64_t after);
+
 /* Per-level profiles of the last cgp_batch_run on this thread (group 0). */
 cgp_status cgp_last_profiles(cgp_level_profile* out, int32_t cap, int32_t* count);
 cgp_status cgp_last_kernel_profile(cgp_kernel_profile* out);
@@ -287,15 +294,15 @@ cgp_status cgp_enactor_read_values(cgp_enactor* e, void* out, int32_t out_layout
  * entries), host `sources` (nq <= 256) and a device output of
  * num_vertices * nq int32 depths, vertex-major out[v*nq + q], INT32_MAX for
  * unreached.  Working state lives in one static device array of
- * CGP_NOALLOC_SCRATCH_BYTES: about 36*V bytes for up to 64 queries and
- * 108*V bytes for up to 256, plus 8 KiB; larger graphs are rejected with
+ * CGP_NOALLOC_SCRATCH_BYTES: about 17 KiB plus 36, 60 or 108 bytes per
+ * vertex for up to 64, 128 or 256 queries; larger graphs are rejected with
  * CGP_ERR_INVALID_ARG.  symmetric != 0 (the CSR holds both directions)
  * allows pull levels; otherwise every level pushes.  The work is enqueued on
  * `stream` (cudaStream_t, NULL = default stream) of the current device and
- * the call returns when it is done.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
- * Calls share the array: calls that overlap on the same device race and must
- * be serialised by the caller. */
+ * the call is synchronous: it waits on `stream` between levels and returns
+ * when the traversal is done.  Every call looks up the array's device
+ * address on the current device.  Calls share the array: calls that overlap
+ * on the same device race and must be serialised by the caller. */
 cgp_status cgp_bfs_batch_noalloc(const void* row_offsets, int32_t offset_bytes,
                                  const int32_t* col_indices, int64_t num_vertices,
                                  int64_t num_edges, const int32_t* sources, int32_t nq,
@@ -375,6 +382,10 @@ cgp_status cgp_pick_sources(const cgp_host_csr* g, int32_t count,
  * (csr_vlist.bin / csr_elist.bin / csr_weightlist.bin, mtx_loader.hxx:189-260). */
 cgp_status cgp_load_matrix_market(const char* path, cgp_host_csr* out);
 cgp_status cgp_load_binary_csr(const char* dir, cgp_host_csr* out);
+/* Galois binary graph, version 1 (load_gr, cgp/examples/algorithms/bfs/cgp_bfs.cu:215-260):
+ * the topology as the reference reads it (unit weights); read_edge_data != 0
+ * keeps 4-byte edge data as uint32 weights. */
+cgp_status cgp_load_galois_gr(const char* path, int32_t read_edge_data, cgp_host_csr* out);
 void cgp_host_csr_free(cgp_host_csr* g);
 
 #ifdef __cplusplus

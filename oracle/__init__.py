@@ -3,9 +3,11 @@
 Loads oracle/liboracle.so (the C restatement in oracle.c of the reference's
 cpu_bfs / cpu_sssp / cpu_wcc, puercgp/examples/mtx_loader.hxx:269-356) and,
 when it was built here, oracle/_ref/libcgpref.so (those same reference
-functions compiled from the reference's own header).  Only the tests,
-__graft_entry__.smoke() and bench.py's CPU-baseline leg use this package; the
-shipped library never does.
+functions compiled from the reference's own header), plus a C restatement
+of the library's seeded graph generators (oracle/gen.c) so that the CPU side
+of the benchmark builds its inputs without loading the product library.  Only
+the tests, __graft_entry__.smoke() and bench.py's CPU legs use this package;
+the shipped library never does.
 """
 from __future__ import annotations
 
@@ -47,8 +49,135 @@ def _load():
         l.oracle_batch.restype = None
         l.oracle_batch.argtypes = [ctypes.c_int32, ctypes.c_int64, P, P, P, P, P, ctypes.c_int32,
                                    ctypes.c_int32, P, P]
+        Csr = ctypes.POINTER(_OracleCsr)
+        l.oracle_gen_rmat.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
+                                      ctypes.c_int32, Csr]
+        l.oracle_gen_grid.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_uint64, Csr]
+        l.oracle_gen_chung_lu.argtypes = [ctypes.c_int64, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_uint64, Csr]
+        l.oracle_gen_weights.argtypes = [Csr, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int32, ctypes.c_uint64]
+        l.oracle_pick_sources.argtypes = [Csr, ctypes.c_int32, ctypes.c_int32, P,
+                                          ctypes.c_uint64, P]
+        l.oracle_csr_from_edges.argtypes = [ctypes.c_int64, ctypes.c_int64, P, P, ctypes.c_int32,
+                                            Csr]
+        l.oracle_csr_free.restype = None
+        l.oracle_csr_free.argtypes = [Csr]
         _lib = l
     return _lib
+
+
+# ------------------------------------------------------------ generators ---
+class _OracleCsr(ctypes.Structure):
+    _fields_ = [("V", ctypes.c_int64), ("E", ctypes.c_int64),
+                ("row", ctypes.POINTER(ctypes.c_int64)), ("col", ctypes.POINTER(ctypes.c_int32)),
+                ("w", ctypes.c_void_p), ("weight_kind", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class Graph:
+    """Host CSR built by the C generators (int64 offsets, int32 columns,
+    optional uint32 / float32 weights)."""
+
+    def __init__(self, row_offsets, col_indices, weights=None):
+        self.row_offsets = row_offsets
+        self.col_indices = col_indices
+        self.weights = weights
+
+    @property
+    def num_vertices(self) -> int:
+        return len(self.row_offsets) - 1
+
+    @property
+    def num_edges(self) -> int:
+        return len(self.col_indices)
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.row_offsets)
+
+    def _c(self):
+        c = _OracleCsr()
+        row, col = _csr(self)
+        self._keep = (row, col)
+        c.V, c.E = len(row) - 1, len(col)
+        c.row = row.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))
+        c.col = col.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        return c
+
+    def with_weights(self, kind: str, p0: float, p1: float, seed: int = 2,
+                     lognormal: bool = False) -> "Graph":
+        c = self._c()
+        wk = 1 if kind == "u32" else 2
+        _check(_load().oracle_gen_weights(ctypes.byref(c), wk, p0, p1, int(lognormal), seed),
+               "oracle_gen_weights")
+        dt = np.uint32 if wk == 1 else np.float32
+        E = self.num_edges
+        w = (np.frombuffer((ctypes.c_char * (4 * max(E, 1))).from_address(c.w), dtype=dt)[:E].copy())
+        c.row = ctypes.POINTER(ctypes.c_int64)()  # arrays owned by numpy
+        c.col = ctypes.POINTER(ctypes.c_int32)()
+        _load().oracle_csr_free(ctypes.byref(c))
+        return Graph(self.row_offsets, self.col_indices, w)
+
+    def pick_sources(self, count: int, seed: int = 42, min_degree: int = 1,
+                     allowed=None) -> np.ndarray:
+        c = self._c()
+        out = np.zeros(count, np.int32)
+        al = None
+        if allowed is not None:
+            allowed = np.ascontiguousarray(allowed, np.uint8)
+            al = allowed.ctypes.data
+        _check(_load().oracle_pick_sources(ctypes.byref(c), count, min_degree, al, seed,
+                                           out.ctypes.data), "oracle_pick_sources")
+        return out
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise (MemoryError if rc == 2 else ValueError)(f"{what} failed ({rc})")
+
+
+def _take(c: _OracleCsr) -> Graph:
+    V, E = c.V, c.E
+    row = np.ctypeslib.as_array(c.row, shape=(V + 1,)).copy()
+    col = np.ctypeslib.as_array(c.col, shape=(max(E, 1),))[:E].copy()
+    _load().oracle_csr_free(ctypes.byref(c))
+    return Graph(row, col)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+             c: float = 0.19, seed: int = 1, permute: bool = True) -> Graph:
+    h = _OracleCsr()
+    _check(_load().oracle_gen_rmat(scale, edge_factor, a, b, c, seed, int(permute),
+                                   ctypes.byref(h)), "oracle_gen_rmat")
+    return _take(h)
+
+
+def gen_grid(rows: int, cols: int, delete_frac: float = 0.1, shortcut_frac: float = 0.001,
+             seed: int = 1) -> Graph:
+    h = _OracleCsr()
+    _check(_load().oracle_gen_grid(rows, cols, delete_frac, shortcut_frac, seed,
+                                   ctypes.byref(h)), "oracle_gen_grid")
+    return _take(h)
+
+
+def gen_chung_lu(num_vertices: int, exponent: float = 2.1, mean_degree: float = 16.0,
+                 seed: int = 1) -> Graph:
+    h = _OracleCsr()
+    _check(_load().oracle_gen_chung_lu(num_vertices, exponent, mean_degree, seed,
+                                       ctypes.byref(h)), "oracle_gen_chung_lu")
+    return _take(h)
+
+
+def csr_from_edges(num_vertices: int, src, dst, symmetrize: bool = True) -> Graph:
+    s = np.ascontiguousarray(src, np.int32)
+    d = np.ascontiguousarray(dst, np.int32)
+    h = _OracleCsr()
+    _check(_load().oracle_csr_from_edges(num_vertices, len(s), s.ctypes.data, d.ctypes.data,
+                                         int(symmetrize), ctypes.byref(h)),
+           "oracle_csr_from_edges")
+    return _take(h)
 
 
 def _csr(g):

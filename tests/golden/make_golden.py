@@ -1,7 +1,7 @@
 """Generates tests/golden/golden.json from the reference.
 
-Run in a container where the reference tree is mounted (default
-/root/reference, or $CGP_REFERENCE):
+Run where the reference tree is available: $CGP_REFERENCE, else a
+directory named `reference` beside the repository:
 
     python tests/golden/make_golden.py
 
@@ -32,7 +32,7 @@ sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402
 import cgp_b200 as cgp  # noqa: E402
 
-REF = Path(os.environ.get("CGP_REFERENCE", "/root/reference"))
+REF = Path(os.environ.get("CGP_REFERENCE", str(ROOT.parent / "reference")))
 INF_I = 2**31 - 1
 
 

@@ -173,3 +173,55 @@ def test_binary_csr_loader(tmp_path):
     np.array([5, 6], np.int32).tofile(tmp_path / "csr_weightlist.bin")
     with pytest.raises(ValueError):
         cgp.load_binary_csr(str(tmp_path))
+
+
+def _write_gr(path, V, rows_end, dst, edge_bytes=0, data=None, version=1):
+    import struct
+    with open(path, "wb") as f:
+        f.write(struct.pack("<4Q", version, edge_bytes, V, len(dst)))
+        f.write(np.asarray(rows_end, np.uint64).tobytes())
+        f.write(np.asarray(dst, np.uint32).tobytes())
+        if data is not None:
+            if len(dst) % 2:
+                f.write(b"\0" * 4)
+            f.write(np.asarray(data, np.uint32).tobytes())
+
+
+def test_galois_gr_loader(tmp_path):
+    # 5 vertices, 7 edges (odd: the edge data follows 4 bytes of padding)
+    rows_end = [2, 3, 3, 6, 7]
+    dst = [1, 3, 2, 0, 1, 4, 0]
+    data = [5, 6, 7, 8, 9, 10, 11]
+    p = tmp_path / "g.gr"
+    _write_gr(p, 5, rows_end, dst, 4, data)
+    g = cgp.load_galois_gr(str(p))  # the reference reads the topology only
+    assert g.row_offsets.tolist() == [0] + rows_end
+    assert g.col_indices.tolist() == dst
+    assert g.weights is None
+    gw = cgp.load_galois_gr(str(p), read_edge_data=True)
+    assert gw.weights.dtype == np.uint32 and gw.weights.tolist() == data
+    # even edge count: no padding
+    p2 = tmp_path / "h.gr"
+    _write_gr(p2, 3, [1, 2, 2], [1, 0], 4, [3, 4])
+    assert cgp.load_galois_gr(str(p2), read_edge_data=True).weights.tolist() == [3, 4]
+
+
+def test_galois_gr_loader_rejects_bad_files(tmp_path):
+    bad = {
+        "version": dict(V=2, rows_end=[1, 1], dst=[1], version=2),
+        "range": dict(V=2, rows_end=[1, 1], dst=[5]),
+        "ends": dict(V=2, rows_end=[1, 3], dst=[1]),
+        "order": dict(V=3, rows_end=[2, 1, 3], dst=[1, 2, 0]),
+    }
+    for name, kw in bad.items():
+        p = tmp_path / f"{name}.gr"
+        _write_gr(p, kw["V"], kw["rows_end"], kw["dst"], version=kw.get("version", 1))
+        with pytest.raises(ValueError):
+            cgp.load_galois_gr(str(p))
+    p = tmp_path / "short.gr"
+    _write_gr(p, 4, [1, 2, 3, 4], [1, 2, 3, 0])
+    p.write_bytes(p.read_bytes()[:-6])
+    with pytest.raises(ValueError, match="truncated"):
+        cgp.load_galois_gr(str(p))
+    with pytest.raises(ValueError):
+        cgp.load_galois_gr(str(tmp_path / "missing.gr"))

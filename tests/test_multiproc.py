@@ -83,3 +83,50 @@ def test_sharded_gather_and_reductions_gloo_world2():
     ok, t, s = q.get(timeout=10)
     assert ok
     assert t == 2.0 and s == 3.0
+
+
+def _cuda_worker(rank, world, port, q):
+    """One rank of the sharded path with the real CUDA runner: every rank
+    runs its shard on cuda:0 (independent processes, no kernel waits on
+    another) and rank 0 gathers the rows over gloo."""
+    import sys
+    from pathlib import Path
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+    import torch.distributed as dist
+
+    import cgp_b200 as cgp
+    import oracle
+    from cgp_b200.parallel import run_sharded
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        cgp.set_device(0)
+        g = cgp.gen_rmat(12, 8, seed=14).with_weights("u32", 1, 16, seed=15)
+        graph = cgp.CsrGraph(g)
+        src = g.pick_sources(37, seed=16)
+        descs = [cgp.QueryDescriptor(int(s), "bfs" if i % 3 else "sssp") for i, s in enumerate(src)]
+        full = run_sharded(graph, descs, rank, world)
+        if rank == 0:
+            exp = np.stack([oracle.bfs(g, d.source).view(np.uint32) if d.kind == "bfs"
+                            else oracle.sssp(g, d.source) for d in descs])
+            q.put(bool(np.array_equal(full, exp)))
+        else:
+            assert full is None
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_sharded_cuda_runner_gloo_world2_one_gpu():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_cuda_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    assert q.get(timeout=10)

@@ -112,3 +112,49 @@ def test_oracle_matches_live_reference_on_random_graphs():
             assert np.array_equal(oracle.sssp(g, int(s)), oracle.ref_sssp(g, int(s)))
         np.testing.assert_array_equal(oracle.wcc_components(g),
                                       oracle.ref_wcc(g).astype(np.uint32))
+
+
+# ------------------------------------------------- generator restatement ---
+# The reference arm of the benchmark builds its inputs with oracle/gen.c; it
+# must produce the library's arrays exactly, or the two arms would time
+# different graphs.
+@pytest.mark.parametrize("scale", [6, 12, 16])
+def test_oracle_rmat_generator_matches_library(scale):
+    import cgp_b200 as cgp
+    a = oracle.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=1)
+    b = cgp.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=1)
+    np.testing.assert_array_equal(a.row_offsets, b.row_offsets)
+    np.testing.assert_array_equal(a.col_indices, b.col_indices)
+    for kind, p0, p1, logn in (("u32", 1, 64, False), ("u32", 1, 255, False),
+                               ("f32", 1.0, 100.0, False), ("f32", 0.0, 1.0, True)):
+        wa = a.with_weights(kind, p0, p1, seed=2, lognormal=logn).weights
+        wb = b.with_weights(kind, p0, p1, seed=2, lognormal=logn).weights
+        assert wa.dtype == wb.dtype
+        np.testing.assert_array_equal(wa.view(np.uint32), wb.view(np.uint32))
+    allowed = (np.arange(a.num_vertices) % 3 == 0).astype(np.uint8)
+    np.testing.assert_array_equal(a.pick_sources(100, seed=42), b.pick_sources(100, seed=42))
+    np.testing.assert_array_equal(a.pick_sources(50, seed=7, allowed=allowed),
+                                  b.pick_sources(50, seed=7, allowed=allowed))
+
+
+def test_oracle_rmat_unpermuted_and_other_params_match_library():
+    import cgp_b200 as cgp
+    a = oracle.gen_rmat(10, 8, 0.45, 0.15, 0.15, seed=9, permute=False)
+    b = cgp.gen_rmat(10, 8, 0.45, 0.15, 0.15, seed=9, permute=False)
+    np.testing.assert_array_equal(a.row_offsets, b.row_offsets)
+    np.testing.assert_array_equal(a.col_indices, b.col_indices)
+
+
+def test_oracle_grid_and_chung_lu_generators_match_library():
+    import cgp_b200 as cgp
+    for a, b in ((oracle.gen_grid(96, 80, 0.1, 0.001, seed=3), cgp.gen_grid(96, 80, 0.1, 0.001, seed=3)),
+                 (oracle.gen_chung_lu(30000, 2.1, 16.0, seed=4),
+                  cgp.gen_chung_lu(30000, 2.1, 16.0, seed=4))):
+        np.testing.assert_array_equal(a.row_offsets, b.row_offsets)
+        np.testing.assert_array_equal(a.col_indices, b.col_indices)
+    src = np.array([0, 1, 1, 2, 5, 5, 7], np.int32)
+    dst = np.array([1, 0, 2, 2, 6, 6, 0], np.int32)
+    a = oracle.csr_from_edges(8, src, dst)
+    b = cgp.csr_from_edges(8, src, dst)
+    np.testing.assert_array_equal(a.row_offsets, b.row_offsets)
+    np.testing.assert_array_equal(a.col_indices, b.col_indices)

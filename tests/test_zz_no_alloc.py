@@ -27,18 +27,21 @@ def _noalloc_fn():
 
 def _run_noalloc(f, row_d, col_d, V, E, sources, out_d, symmetric, stream):
     src = np.ascontiguousarray(sources, np.int32)
-    st = f(row_d.data_ptr(), 4, col_d.data_ptr(), V, E, src.ctypes.data, len(src), symmetric,
+    ob = row_d.element_size()
+    st = f(row_d.data_ptr(), ob, col_d.data_ptr(), V, E, src.ctypes.data, len(src), symmetric,
            out_d.data_ptr(), stream)
     N.check(st, "cgp_bfs_batch_noalloc")
 
 
-@pytest.mark.parametrize("nq,symmetric", [(64, 1), (200, 0)])
-def test_noalloc_matches_regular_entry_point_twice(nq, symmetric):
+# (queries, symmetric, offset bytes): one, two and four mask words; 32- and
+# 64-bit row offsets
+@pytest.mark.parametrize("nq,symmetric,ob", [(64, 1, 4), (200, 0, 4), (100, 1, 8), (30, 0, 8)])
+def test_noalloc_matches_regular_entry_point_twice(nq, symmetric, ob):
     import torch
     g = cgp.gen_rmat(14, 8, seed=301)
     V, E = g.num_vertices, g.num_edges
     dev = torch.device("cuda", 0)
-    row_d = torch.from_numpy(g.row_offsets.astype(np.int32)).to(dev)
+    row_d = torch.from_numpy(g.row_offsets.astype(np.int32 if ob == 4 else np.int64)).to(dev)
     col_d = torch.from_numpy(g.col_indices).to(dev)
     graph = cgp.CsrGraph(g)
     f = _noalloc_fn()
@@ -50,7 +53,7 @@ def test_noalloc_matches_regular_entry_point_twice(nq, symmetric):
         free_before = torch.cuda.mem_get_info(dev)[0]
         _run_noalloc(f, row_d, col_d, V, E, src, out, symmetric, stream)
         torch.cuda.synchronize(dev)
-        if call == 1:  # the scratch array was set up by the first call
+        if call == 1:  # the first call may have loaded the library's device module
             assert torch.cuda.mem_get_info(dev)[0] == free_before
         np.testing.assert_array_equal(out.cpu().numpy(), expect)
 
