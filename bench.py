@@ -102,6 +102,8 @@ def parse_args():
     p.add_argument("--heavy-degree", type=int, default=0)
     p.add_argument("--sssp-pull-edge-ratio", type=float, default=0.5)
     p.add_argument("--levels-per-sync", type=int, default=0)
+    p.add_argument("--level-loop", default="", choices=["", "auto", "chunks", "device"],
+                   help="level loop form (default: device-looped graph for c3, else chunks)")
     p.add_argument("--no-light-chunks", action="store_true",
                    help="gather light vertices one warp per vertex instead of in CTA chunks")
     p.add_argument("--no-autotune", action="store_true")
@@ -112,6 +114,8 @@ def parse_args():
     p.add_argument("--serve-rates", default="500,2000,8000")
     p.add_argument("--serve-seconds", type=float, default=3.0)
     p.add_argument("--serve-slots", type=int, default=256)
+    p.add_argument("--sssp-chunk-direction", type=int, default=0,
+                   help="SSSP gather/scatter per 32-slot chunk (1), per group (-1), auto (0)")
     p.add_argument("--serve-profile", action="store_true",
                    help="time the serving loop's kernel classes (slower: no CUDA graphs)")
     a = p.parse_args()
@@ -571,6 +575,7 @@ def run_serve(args):
                     options=cgp.RunOptions(traversal_mode=args.mode,
                                            pull_edge_ratio=args.pull_edge_ratio,
                                            heavy_degree=args.heavy_degree,
+                                           sssp_chunk_direction=args.sssp_chunk_direction,
                                            profile_kernels=args.serve_profile)) as srv:
         poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
@@ -590,6 +595,8 @@ def run_serve(args):
     line = {"metric": "serve p50/p99 latency", "unit": "ms", "workload":
             f"rmat{scale}_serving_mix60_30_10", "V": g.num_vertices, "E": g.num_edges,
             "offsets": "int64", "slots": st["slots"], "state_bytes": st["state_bytes"],
+            "sssp_direction": {1: "per 32-slot chunk", -1: "per group"}.get(
+                args.sssp_chunk_direction, "auto (per 32-slot chunk)"),
             "seconds_per_rate": args.serve_seconds, "rates": rows, "graph_gen_s": gen_s}
     print(json.dumps(line), flush=True)
     if args.json_out:
@@ -670,7 +677,8 @@ def main():
     tuning = dict(traversal_mode=args.mode, pull_edge_ratio=args.pull_edge_ratio,
                   pull_frontier_ratio=args.pull_frontier_ratio, heavy_degree=args.heavy_degree,
                   sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
-                  light_chunks=not args.no_light_chunks, levels_per_sync=args.levels_per_sync)
+                  light_chunks=not args.no_light_chunks, levels_per_sync=args.levels_per_sync,
+                  level_loop=args.level_loop or ("device" if args.workload == "c3" else "chunks"))
     base = cgp.RunOptions(stream=stream.cuda_stream, **tuning)
     if args.workload == "c5":
         # 1024-slot groups; depths written at discovery into the output, which
@@ -680,12 +688,15 @@ def main():
     if args.workload == "c3":
         base = dataclasses.replace(base, mask_words=16)
 
-    # outputs: one device buffer per distinct group shape (c5's four groups share one)
-    outs = {}
+    # outputs: one device buffer per group, except that c5's four 1024-slot
+    # groups share one (137 GB each): every group's values are written, the
+    # next group's run overwrites them
+    outs = []
     for k, src in groups:
-        key = (len(src),)
-        if key not in outs:
-            outs[key] = torch.empty((V, len(src)), dtype=torch.int32, device=dev)
+        if args.workload == "c5" and outs:
+            outs.append(outs[0])
+        else:
+            outs.append(torch.empty((V, len(src)), dtype=torch.int32, device=dev))
     out_w = torch.empty((V, 1), dtype=torch.int32, device=dev) if wl["wcc"] else None
     wcc_d = [cgp.QueryDescriptor(0, "wcc")]
 
@@ -705,8 +716,8 @@ def main():
 
     def step():
         res = []
-        for d, o, (k, src) in zip(descs, opts, groups):
-            res.append(cgp.run_batch(graph, d, o, out=outs[(len(src),)]))
+        for d, o, out in zip(descs, opts, outs):
+            res.append(cgp.run_batch(graph, d, o, out=out))
         if wl["wcc"]:
             res.append(cgp.run_batch(graph, wcc_d, base, out=out_w))
         return res
@@ -715,7 +726,7 @@ def main():
     for w in range(max(3, args.warmup)):
         if w == 0:
             for gi, (d, o, (k, src)) in enumerate(zip(descs, opts, groups)):
-                out = outs[(len(src),)]
+                out = outs[gi]
                 cgp.run_batch(graph, d, o, out=out)
                 got = reached_counts(out, k, wk)
                 assert np.array_equal(got, expect_reach[gi]), (args.workload, k, gi)
@@ -767,7 +778,7 @@ def main():
         for i, (d, o, (k, src)) in enumerate(zip(descs, opts, groups)):
             p = cgp.run_batch(graph, d, dataclasses.replace(o, profile_kernels=True,
                                                             profile_iterations=True),
-                              out=outs[(len(src),)])
+                              out=outs[i])
             qs = len(d) if k == "sssp" else 0
             merge_classes(kclass, level_classes(p.iteration_profiles, k, V, p.mask_words, qs=qs))
             if k == "bfs":
@@ -864,8 +875,8 @@ def main():
             col = (lambda j: hv[j]) if qmaj else (lambda j: hv[:, j])
             same = True
             j0 = 0
-            for (k, src) in groups:
-                dev_out = outs[(len(src),)]
+            for gi, (k, src) in enumerate(groups):
+                dev_out = outs[gi]
                 if args.workload != "c5":
                     for j in (0, len(src) - 1):
                         same &= bool(np.array_equal(col(j0 + j), dev_out[:, j].cpu().numpy()))
@@ -898,7 +909,7 @@ def main():
         dt, edges, kind, couts = cpu_reference_sample(g, groups, sizes, threads)
         match = True
         for gi, ((k, src), n, co) in enumerate(zip(groups, sizes, couts)):
-            out = outs[(len(src),)]
+            out = outs[gi]
             if args.workload == "c5":  # groups share one output: re-run this one
                 cgp.run_batch(graph, descs[gi], opts[gi], out=out)
             got = out[:, :n].cpu().numpy().T.copy()
@@ -917,7 +928,7 @@ def main():
             "ms_per_step": ms_max / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": wk or "i32", "data": "synthetic",
             "config": workload_config(args, wl, g, world),
-            "engine": {"traversal_mode": args.mode,
+            "engine": {"traversal_mode": args.mode, "level_loop": base.level_loop,
                        "options": [{"kind": k, "mask_words": o.mask_words,
                                     "heavy_degree": o.heavy_degree,
                                     "pull_edge_ratio": o.pull_edge_ratio,

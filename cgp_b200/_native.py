@@ -21,6 +21,7 @@ MODE_PUSH, MODE_PULL, MODE_HYBRID = range(3)
 WEIGHT_NONE, WEIGHT_U32, WEIGHT_F32 = range(3)
 LAYOUT_VERTEX_MAJOR, LAYOUT_QUERY_MAJOR = range(2)
 DEPTH_AUTO, DEPTH_PLANES, DEPTH_DIRECT = range(3)
+LOOP_AUTO, LOOP_CHUNKS, LOOP_DEVICE = range(3)
 GRAPH_DEVICE_POINTERS, GRAPH_SYMMETRIC, GRAPH_OFFSETS64 = 1, 2, 4
 BFS_UNREACHED = 2**31 - 1
 U32_UNREACHED = 2**32 - 1
@@ -38,8 +39,8 @@ class CgpOptions(Structure):
         ("use_cuda_graph", c_int32), ("levels_per_sync", c_int32), ("mask_words", c_int32),
         ("depth_mode", c_int32), ("heavy_degree", c_int32), ("max_queries", c_int32),
         ("discard_results", c_int32), ("profile_kernels", c_int32), ("dense_unroll", c_int32),
-        ("sssp_pull_edge_ratio", c_double), ("light_chunks", c_int32), ("reserved", c_int32),
-        ("stream", c_void_p),
+        ("sssp_pull_edge_ratio", c_double), ("light_chunks", c_int32), ("level_loop", c_int32),
+        ("sssp_chunk_direction", c_int32), ("reserved", c_int32), ("stream", c_void_p),
     ]
 
 

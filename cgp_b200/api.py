@@ -296,6 +296,8 @@ class RunOptions:
     dense_unroll: int = 0
     sssp_pull_edge_ratio: float = 0.5
     light_chunks: bool = True
+    level_loop: str = "auto"    # "auto", "chunks" (host-checked graph chunks), "device"
+    sssp_chunk_direction: int = 0  # 1 per 32-slot chunk, -1 whole group, 0 auto (serving: chunk)
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -319,6 +321,11 @@ class RunOptions:
         o.dense_unroll = self.dense_unroll
         o.sssp_pull_edge_ratio = self.sssp_pull_edge_ratio
         o.light_chunks = 0 if self.light_chunks else -1
+        if self.level_loop not in ("auto", "chunks", "device"):
+            raise ValueError("level_loop must be auto, chunks or device")
+        o.level_loop = {"auto": N.LOOP_AUTO, "chunks": N.LOOP_CHUNKS,
+                        "device": N.LOOP_DEVICE}[self.level_loop]
+        o.sssp_chunk_direction = int(self.sssp_chunk_direction)
         o.stream = self.stream or None
         return o
 

@@ -25,6 +25,7 @@ enum : int32_t { kWeightNone = 0, kWeightU32 = 1, kWeightF32 = 2 };
 // status bits reported back to the host
 enum : uint32_t {
   kStatusPlanesExhausted = 1u,  // depth planes too few for the level reached
+  kStatusLevelCap = 2u,         // a device-looped traversal reached its level cap
 };
 
 struct LevelProfile {
@@ -69,6 +70,12 @@ struct LevelCtl {
   uint64_t expand[kMaxW];       // bits allowed to expand at the current level
   uint64_t bfs_bits[kMaxW];     // slots with visited-mask semantics (BFS, k-hop)
   uint64_t sssp_bits[kMaxW];    // slots with min-reduce semantics (SSSP)
+  uint64_t gsel[kMaxW];         // SSSP slots that gather (pull) at the current level
+  uint64_t ssel[kMaxW];         // SSSP slots that scatter (push) at the current level
+  unsigned long long cedges[2 * kMaxW];  // per 32-slot chunk: out-edges of the next
+                                         // frontier's vertices with an SSSP bit in it
+  int32_t sscatter;             // ssel has a bit: the scatter kernels have work
+  int32_t chunk_dir;            // SSSP direction decided per 32-slot chunk
   int32_t level;
   int32_t dir;                  // BFS direction of the current level
   int32_t sdir;                 // SSSP direction: push (scatter) or pull (gather)

@@ -346,6 +346,10 @@ struct LevelLaunch {
   bool lchunks;      // light vertices gathered in CTA chunks (W <= 4)
   int dense_unroll;  // edges per step of the dense SSSP kernel (1 or 2)
   KernelTimer* kt;   // per-class event timing (non-graph runs only)
+  bool chunk_dir = false;                 // census of per-chunk frontier edges
+  bool device_loop = false;               // level end sets a WHILE node's condition
+  cudaGraphConditionalHandle loop = 0;    // ... this one
+  int32_t level_cap = 0;                  // ... and stops at this many levels
 };
 
 template <typename K>
@@ -439,7 +443,12 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
 
   }
   if (kt) kt->mark(kClassLevelEnd, s);
-  k_level_end<W><<<1, 32, 0, s>>>(L.g);
+  if (L.chunk_dir) {
+    k_chunk_census<W, OT><<<c, kBlock, 0, s>>>(L.g, L.G);
+    ++n;
+  }
+  if (L.device_loop) k_level_end_loop<W><<<1, 32, 0, s>>>(L.g, L.loop, L.level_cap);
+  else k_level_end<W><<<1, 32, 0, s>>>(L.g);
   ++n;
   if (kt) kt->mark(-1, s);
   return n;
@@ -556,6 +565,13 @@ bool sssp_gather_on(const GraphImpl* g, const cgp_options& o) {
   return o.traversal_mode == CGP_MODE_PULL || o.sssp_pull_edge_ratio > 0;
 }
 
+// SSSP direction per 32-slot chunk: asked for, or by default in serving
+// groups (whose slots are in every phase of their traversals at once).
+bool sssp_chunk_dir(const GroupSpec& spec, const cgp_options& o) {
+  if (!spec.has_sssp || o.traversal_mode != CGP_MODE_HYBRID) return false;
+  return o.sssp_chunk_direction > 0 || (o.sssp_chunk_direction == 0 && spec.serving);
+}
+
 }  // namespace
 
 void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
@@ -631,6 +647,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   c.pull_edge_threshold = static_cast<unsigned long long>(
       std::max(1.0, o.pull_edge_ratio * static_cast<double>(g->E)));
   c.sssp_gather = sssp_gather_on(g, o) ? 1 : 0;
+  c.chunk_dir = sssp_chunk_dir(spec, o) ? 1 : 0;
   c.sssp_pull_edge_threshold = static_cast<unsigned long long>(
       std::max(1.0, o.sssp_pull_edge_ratio * static_cast<double>(g->E)));
   ck(cudaMemcpyAsync(ws->ctl.p, &c, sizeof(LevelCtl), cudaMemcpyHostToDevice, s), "upload ctl");
@@ -652,7 +669,10 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
 
 namespace {
 
-// Enqueues `levels` levels either as a replayed CUDA graph or as plain launches.
+// Enqueues `levels` levels either as a replayed CUDA graph or as plain
+// launches; levels < 0: the whole traversal as one device-looped graph (a
+// WHILE conditional node around one level, the condition set by the level's
+// last kernel from the done flag).
 int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp_options& o,
                    cudaStream_t s, int levels, KernelTimer* kt) {
   Dispatch d = dispatch(spec.W, g->offset_bytes, spec.depth_mode, g->weight_kind);
@@ -674,6 +694,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
     L.lchunks = spec.W <= 4 && o.light_chunks >= 0;
   }
   L.dense_unroll = o.dense_unroll == 2 ? 2 : 1;
+  L.chunk_dir = L.spull && sssp_chunk_dir(spec, o);
   L.kt = kt;
   if (!o.use_cuda_graph || kt != nullptr) {
     int n = 0;
@@ -682,25 +703,59 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
     return n;
   }
   L.kt = nullptr;
+  const bool loop = levels < 0;
   auto key = std::make_tuple(spec.W, g->offset_bytes, spec.depth_mode, g->weight_kind,
                              (spec.has_bfs ? 1 : 0) | (spec.has_sssp ? 2 : 0) | (L.pull ? 4 : 0) |
                                  (o.profile_iterations ? 8 : 0) | (L.dense_unroll == 2 ? 16 : 0) |
-                                 (L.spull ? 32 : 0) | (L.lchunks ? 64 : 0),
+                                 (L.spull ? 32 : 0) | (L.lchunks ? 64 : 0) | (loop ? 128 : 0) |
+                                 (L.chunk_dir ? 256 : 0),
                              levels, spec.Qg, static_cast<int>(L.G.heavy_degree), ws->generation,
                              reinterpret_cast<uint64_t>(L.g.values));
   auto it = ws->graphs.find(key);
   if (it == ws->graphs.end()) {
     cudaGraph_t graph = nullptr;
     int n = 0;
-    ck(cudaStreamBeginCapture(ws->capture, cudaStreamCaptureModeThreadLocal), "begin capture");
-    for (int i = 0; i < levels; ++i) n += d.enqueue(L, ws->capture);
-    cudaError_t le = cudaGetLastError();
-    cudaError_t ce = cudaStreamEndCapture(ws->capture, &graph);
-    ck(le, "capture launch");
-    ck(ce, "end capture");
+    if (loop) {
+      ck(cudaGraphCreate(&graph, 0), "graph create");
+      try {
+        cudaGraphConditionalHandle h = 0;
+        ck(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault),
+           "conditional handle");
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        ck(cudaGraphAddNode(&node, graph, nullptr, 0, &p), "conditional node");
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        L.device_loop = true;
+        L.loop = h;
+        L.level_cap = static_cast<int32_t>(std::min<int64_t>(g->V + 2, INT32_MAX - 1));
+        ck(cudaStreamBeginCaptureToGraph(ws->capture, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal),
+           "begin capture");
+        n = d.enqueue(L, ws->capture);
+        cudaError_t le = cudaGetLastError();
+        cudaError_t ce = cudaStreamEndCapture(ws->capture, &body);
+        ck(le, "capture launch");
+        ck(ce, "end capture");
+      } catch (...) {
+        cudaGraphDestroy(graph);
+        throw;
+      }
+    } else {
+      ck(cudaStreamBeginCapture(ws->capture, cudaStreamCaptureModeThreadLocal), "begin capture");
+      for (int i = 0; i < levels; ++i) n += d.enqueue(L, ws->capture);
+      cudaError_t le = cudaGetLastError();
+      cudaError_t ce = cudaStreamEndCapture(ws->capture, &graph);
+      ck(le, "capture launch");
+      ck(ce, "end capture");
+    }
     cudaGraphExec_t exec = nullptr;
-    ck(cudaGraphInstantiate(&exec, graph, 0), "instantiate");
+    cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
+    ck(ie, "instantiate");
     it = ws->graphs.emplace(key, CachedGraph{exec, n}).first;
   }
   ck(cudaGraphLaunch(it->second.exec, s), "graph launch");
@@ -715,7 +770,20 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
   int enqueued = 0;
   int chunk = 0;
   LevelCtl* snap = ws->hctl;
+  // A run to convergence without per-level timing is one device-looped graph:
+  // the host waits once.  (The launch count of such a run is that of one
+  // level; the per-level count is reported with the level count below.)
+  const bool device_loop = kt == nullptr && max_levels <= 0 && o.use_cuda_graph &&
+                           o.level_loop == CGP_LOOP_DEVICE;
+  if (device_loop) {
+    const int per_level = enqueue_levels(g, ws, spec, o, s, -1, nullptr);
+    ck(cudaStreamSynchronize(s), "device level loop");
+    LevelCtl c;
+    ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
+    spec.launches += static_cast<uint64_t>(per_level) * static_cast<uint64_t>(std::max(1, c.level));
+  }
   for (;;) {
+    if (device_loop) break;
     int n = per_chunk;
     if (max_levels > 0) n = std::min(n, max_levels - enqueued);
     if (n <= 0) break;
@@ -750,6 +818,9 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
   ck(cudaStreamSynchronize(s), "level loop");
   LevelCtl c;
   ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
+  if (c.status & kStatusLevelCap)
+    throw ApiError{CGP_ERR_DEVICE, "traversal did not converge within " +
+                                       std::to_string(c.level) + " levels"};
   if (c.done == 2 && (c.status & kStatusPlanesExhausted)) {
     // Deeper than the depth planes can hold: grow them and resume.
     const size_t mask_bytes = static_cast<size_t>(g->V) * spec.W * 8;

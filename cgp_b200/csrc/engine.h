@@ -174,6 +174,7 @@ struct GroupSpec {
   bool has_sssp = false;
   uint32_t* external_values = nullptr;  // caller's device buffer used as working values
   uint32_t uniform_inf = 0;             // nonzero: fill every value with it (serving)
+  bool serving = false;                 // the group belongs to a serving loop
   uint64_t launches = 0;                // kernels enqueued for this group
 };
 

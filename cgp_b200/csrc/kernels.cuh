@@ -434,7 +434,7 @@ constexpr int kQueueShift = 40;
 template <typename OT>
 __global__ void __launch_bounds__(kBlock) k_heavy_queue(GroupDev g, DevGraph G) {
   LevelCtl* ctl = g.ctl;
-  if (ctl->done || (ctl->dir != kDirPush && ctl->sdir != kDirPush)) return;
+  if (ctl->done || (ctl->dir != kDirPush && !ctl->sscatter)) return;
   const LevelView lv = level_view(g);
   const unsigned long long n = ctl->count[lv.par];
   for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -963,7 +963,7 @@ __device__ __forceinline__ void sssp_dense_edges(const GroupDev& g, const DevGra
 template <int W, typename OT, int WK, int U>
 __global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done || ctl->sdir != kDirPush) return;
+  if (ctl->done || !ctl->sscatter) return;
   const LevelView lv = level_view(g);
   WarpAppender ap;
   const unsigned long long n = ctl->dense_count;
@@ -981,7 +981,7 @@ __global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDe
     uint64_t b[W];
     load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
 #pragma unroll
-    for (int k = 0; k < W; ++k) b[k] &= ctl->sssp_bits[k];
+    for (int k = 0; k < W; ++k) b[k] &= ctl->ssel[k];
     sssp_dense_edges<W, OT, WK, U>(g, G, lv, u, b, beg, end, lane, uni, improved, ap);
   }
   ap.flush<OT>(G, lv, lane);
@@ -995,13 +995,13 @@ __global__ void __launch_bounds__(kBlock, (U == 1 ? 4 : 3)) k_sssp_dense(GroupDe
 template <int W, typename OT, int WK>
 __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done || ctl->sdir != kDirPush) return;
+  if (ctl->done || !ctl->sscatter) return;
   const LevelView lv = level_view(g);
   WarpAppender ap;
   const unsigned long long n = ctl->count[lv.par];
   uint64_t sel[W];
 #pragma unroll
-  for (int i = 0; i < W; ++i) sel[i] = ctl->sssp_bits[i];
+  for (int i = 0; i < W; ++i) sel[i] = ctl->ssel[i];
   if (!mask_any<W>(sel)) return;
   __shared__ int64_t s_beg[kWarpsPerBlock][32];
   __shared__ long long s_inc[kWarpsPerBlock][32];
@@ -1120,7 +1120,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
 template <int W, typename OT, int WK>
 __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done || ctl->sdir != kDirPush) return;
+  if (ctl->done || !ctl->sscatter) return;
   const unsigned long long hq = ctl->hq_packed;
   const int nq = static_cast<int>(hq >> kQueueShift);
   const int64_t nchunks = static_cast<int64_t>(hq & ((1ULL << kQueueShift) - 1));
@@ -1144,7 +1144,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
     uint64_t b[W];
     load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, b);
 #pragma unroll
-    for (int i = 0; i < W; ++i) b[i] &= ctl->sssp_bits[i];
+    for (int i = 0; i < W; ++i) b[i] &= ctl->ssel[i];
     if (threadIdx.x == 0) {
       int acc = 0;
       for (int i = 0; i < W; ++i) {
@@ -1262,13 +1262,14 @@ struct GatherSteps {
   static constexpr int value = W >= 16 ? 1 : (W >= 8 ? 2 : (W >= 4 ? 4 : 8));
 };
 
-// Bit c of the result: this lane's slot of chunk c is an SSSP slot.
+// Bit c of the result: this lane's slot of chunk c is an SSSP slot that
+// gathers at this level.
 template <int W>
 __device__ __forceinline__ uint32_t lane_sssp_chunks(const LevelCtl* ctl, int lane) {
   uint32_t sel = 0;
 #pragma unroll
   for (int c = 0; c < 2 * W; ++c)
-    sel |= static_cast<uint32_t>((ctl->sssp_bits[c >> 1] >> (32 * (c & 1) + lane)) & 1ULL) << c;
+    sel |= static_cast<uint32_t>((ctl->gsel[c >> 1] >> (32 * (c & 1) + lane)) & 1ULL) << c;
   return sel;
 }
 
@@ -1338,7 +1339,7 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 2)) k_sssp_pull(GroupDev
   const LevelView lv = level_view(g);
   constexpr int C = 2 * W;
   const int lane = threadIdx.x & 31;
-  const uint64_t* sb = ctl->sssp_bits;
+  const uint64_t* sb = ctl->gsel;
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
   const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
@@ -1402,7 +1403,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy(GroupDev g, DevGraph
   __shared__ int32_t s_h;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const uint64_t* sb = ctl->sssp_bits;
+  const uint64_t* sb = ctl->gsel;
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
   const size_t Qg = static_cast<size_t>(g.Qg);
   uint64_t uni[W];
@@ -1534,8 +1535,10 @@ __device__ __forceinline__ void relax_min_row(uint32_t (&best)[N], const uint32_
 }
 
 // Lane masks for the vectorised gather: bit r of *parts: the lane's vector of
-// part r lies inside the row (slot < Qg); bit j of *slots: slot j of the lane
-// is an SSSP slot.
+// part r lies inside the row (slot < Qg) and holds a slot that gathers at this
+// level (otherwise the lane neither loads nor commits it: a 32-slot chunk
+// without gathering slots is never read); bit j of *slots: slot j of the lane
+// gathers.
 template <int W>
 __device__ __forceinline__ void gather_vec_masks(const LevelCtl* ctl, int Qg, int lane,
                                                  uint32_t* parts, uint32_t* slots) {
@@ -1544,12 +1547,12 @@ __device__ __forceinline__ void gather_vec_masks(const LevelCtl* ctl, int Qg, in
 #pragma unroll
   for (int r = 0; r < GV::kParts; ++r) {
     const int base = (32 * r + lane) * GV::kElem;
-    if (base < Qg) pm |= 1u << r;
 #pragma unroll
     for (int k = 0; k < GV::kElem; ++k) {
       const int q = base + k;
-      if (q < Qg && ((ctl->sssp_bits[q >> 6] >> (q & 63)) & 1ULL)) sm |= 1u << (r * GV::kElem + k);
+      if (q < Qg && ((ctl->gsel[q >> 6] >> (q & 63)) & 1ULL)) sm |= 1u << (r * GV::kElem + k);
     }
+    if (base < Qg && ((sm >> (r * GV::kElem)) & ((1u << GV::kElem) - 1u))) pm |= 1u << r;
   }
   *parts = pm;
   *slots = sm;
@@ -1587,7 +1590,7 @@ __device__ __forceinline__ int gather_screen_qs(const LevelCtl* ctl, const Level
                                                 int64_t E) {
   int qs = 0;
 #pragma unroll
-  for (int i = 0; i < W; ++i) qs += __popcll(ctl->sssp_bits[i]);
+  for (int i = 0; i < W; ++i) qs += __popcll(ctl->gsel[i]);
   if (2 * ctl->edges[lv.par] < static_cast<unsigned long long>(E)) return -1;
   if (32 * ctl->prev_improved < ctl->count[lv.par] * static_cast<unsigned long long>(qs)) return -1;
   return qs;
@@ -1725,7 +1728,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   const LevelView lv = level_view(g);
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const uint64_t* sb = ctl->sssp_bits;
+  const uint64_t* sb = ctl->gsel;
   uint32_t pmask, smask;
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -1852,7 +1855,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
   __shared__ int32_t s_pre[kLightChunkVerts + 1];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const uint64_t* sb = ctl->sssp_bits;
+  const uint64_t* sb = ctl->gsel;
   uint32_t pmask, smask;
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
@@ -2069,7 +2072,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   __shared__ int32_t s_h;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const uint64_t* sb = ctl->sssp_bits;
+  const uint64_t* sb = ctl->gsel;
   uint32_t pmask, smask;
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
@@ -2176,6 +2179,38 @@ __device__ __forceinline__ bool any_bits(const uint64_t* m) {
   return a != 0;
 }
 
+// Splits the SSSP slots of the next level into gathering (gsel) and
+// scattering (ssel) ones.  Group-wide by default (every slot takes
+// `group_dir`); with chunk_dir in hybrid mode each 32-slot chunk gathers when
+// the out-edges of the next frontier's vertices that carry one of its bits
+// (cedges, summed by k_chunk_census) reach the gather threshold, so a few
+// queries in their dense phase do not make every other slot gather too.
+// Consumes (zeroes) cedges.
+template <int W>
+__device__ __forceinline__ void split_sssp_slots(LevelCtl* ctl, int32_t group_dir) {
+  const bool per_chunk = ctl->chunk_dir && ctl->mode == 2 && ctl->forced_dir < 0 &&
+                         ctl->sssp_gather;
+  bool g_any = false, s_any = false;
+  for (int i = 0; i < W; ++i) {
+    uint64_t gm = 0;
+    if (per_chunk) {
+      for (int h = 0; h < 2; ++h) {
+        const uint64_t half = 0xffffffffULL << (32 * h);
+        if (ctl->cedges[2 * i + h] >= ctl->sssp_pull_edge_threshold) gm |= half;
+      }
+    } else if (group_dir == kDirPull) {
+      gm = ~0ULL;
+    }
+    ctl->gsel[i] = ctl->sssp_bits[i] & gm;
+    ctl->ssel[i] = ctl->sssp_bits[i] & ~gm;
+    g_any |= ctl->gsel[i] != 0;
+    s_any |= ctl->ssel[i] != 0;
+  }
+  for (int c = 0; c < 2 * kMaxW; ++c) ctl->cedges[c] = 0;
+  ctl->sdir = g_any ? kDirPull : kDirPush;
+  ctl->sscatter = s_any ? 1 : 0;
+}
+
 // Expand mask for `level`: k-hop slots stop once their depth reaches k.
 template <int W>
 __device__ void compute_expand(LevelCtl* ctl, const SlotDev* slots, int Qg, int level) {
@@ -2189,9 +2224,9 @@ __device__ void compute_expand(LevelCtl* ctl, const SlotDev* slots, int Qg, int 
 // End of a level (one thread): profile, convergence, and the set-up of the
 // next level (counter reset, direction, expand mask).
 template <int W>
-__global__ void k_level_end(GroupDev g) {
+__device__ void level_end(GroupDev& g) {
   LevelCtl* ctl = g.ctl;
-  if (ctl->done || threadIdx.x != 0) return;
+  if (ctl->done) return;
   const int l = ctl->level;
   const int par = l & 1;
   const unsigned long long nextc = ctl->count[par ^ 1];
@@ -2240,7 +2275,7 @@ __global__ void k_level_end(GroupDev g) {
   for (int i = 0; i < W; ++i) ctl->active[par][i] = 0;
   compute_expand<W>(ctl, g.slots, g.Qg, l + 1);
   ctl->dir = decide_dir(ctl, nextc, ctl->edges[par ^ 1], any_bits<W>(ctl->bfs_bits));
-  ctl->sdir = decide_sdir(ctl, ctl->edges[par ^ 1], any_bits<W>(ctl->sssp_bits));
+  split_sssp_slots<W>(ctl, decide_sdir(ctl, ctl->edges[par ^ 1], any_bits<W>(ctl->sssp_bits)));
   if (nextc == 0 || (ctl->max_iterations > 0 && l + 1 >= ctl->max_iterations)) {
     ctl->done = 1;
     return;
@@ -2253,6 +2288,68 @@ __global__ void k_level_end(GroupDev g) {
     ctl->done = 2;
   }
   if (ctl->halt_level >= 0 && l + 1 >= ctl->halt_level) ctl->done = 2;
+}
+
+template <int W>
+__global__ void k_level_end(GroupDev g) {
+  if (threadIdx.x == 0) level_end<W>(g);
+}
+
+// Per 32-slot chunk, the out-edges of the next frontier's vertices that carry
+// an SSSP bit of the chunk (input of the per-chunk direction decision).  Runs
+// after the level's kernels, before its level end: each lane takes a vertex
+// of the next frontier list, the warp sums its chunks, lane 0 adds them.
+template <int W, typename OT>
+__global__ void __launch_bounds__(kBlock) k_chunk_census(GroupDev g, DevGraph G) {
+  LevelCtl* ctl = g.ctl;
+  if (ctl->done || !ctl->chunk_dir) return;
+  const LevelView lv = level_view(g);
+  const unsigned long long n = *lv.ncount;
+  const int lane = threadIdx.x & 31;
+  unsigned long long acc[2 * W];
+#pragma unroll
+  for (int c = 0; c < 2 * W; ++c) acc[c] = 0;
+  const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  for (unsigned long long i0 = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
+       i0 < n; i0 += stride) {
+    const unsigned long long i = i0 + lane;
+    if (i < n) {
+      const int32_t v = lv.nlist[i];
+      const unsigned long long d = degree_of<OT>(G.row, v);
+      uint64_t m[W];
+      load_mask<W>(lv.fnext + static_cast<size_t>(v) * W, m);
+#pragma unroll
+      for (int w = 0; w < W; ++w) {
+        const uint64_t x = m[w] & ctl->sssp_bits[w];
+        if (static_cast<uint32_t>(x)) acc[2 * w] += d;
+        if (static_cast<uint32_t>(x >> 32)) acc[2 * w + 1] += d;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 2 * W; ++c) {
+    unsigned long long x = acc[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+    if (lane == 0 && x) atomicAdd(&ctl->cedges[c], x);
+  }
+}
+
+// Level end inside a device-looped CUDA graph (a WHILE conditional node whose
+// body is one level): sets the loop condition from the done flag, so the
+// whole traversal runs without the host.  A traversal that is still running
+// at `level_cap` levels (more than any converging BFS/SSSP needs) stops with
+// kStatusLevelCap instead of looping on.
+template <int W>
+__global__ void k_level_end_loop(GroupDev g, cudaGraphConditionalHandle loop, int32_t level_cap) {
+  if (threadIdx.x != 0) return;
+  level_end<W>(g);
+  LevelCtl* ctl = g.ctl;
+  if (ctl->done == 0 && ctl->level >= level_cap) {
+    ctl->status |= kStatusLevelCap;
+    ctl->done = 3;
+  }
+  cudaGraphSetConditional(loop, ctl->done == 0 ? 1u : 0u);
 }
 
 // Seeds the sources of every slot (one block).  Level 0 starts afterwards.
@@ -2289,7 +2386,8 @@ __global__ void k_seed(GroupDev g, DevGraph G) {
   if (threadIdx.x == 0) {
     compute_expand<W>(ctl, g.slots, g.Qg, 0);
     ctl->dir = decide_dir(ctl, ctl->count[0], ctl->edges[0], any_bits<W>(ctl->bfs_bits));
-    ctl->sdir = decide_sdir(ctl, ctl->edges[0], any_bits<W>(ctl->sssp_bits));
+    // the sources' level: every slot starts with the group's direction
+    split_sssp_slots<W>(ctl, decide_sdir(ctl, ctl->edges[0], any_bits<W>(ctl->sssp_bits)));
     if (ctl->count[0] == 0) ctl->done = 1;
   }
 }

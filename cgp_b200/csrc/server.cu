@@ -75,12 +75,17 @@ __global__ void k_admit(GroupDev g, DevGraph G, const AdmitReq* reqs, int n) {
       sd.base = L;
       slots[s] = sd;
       const bool bfs_like = r.kind == 0 || r.kind == 3;
+      // a new SSSP slot scatters from its source until the level ends decide
+      // its chunk's direction again
+      atomicAnd(reinterpret_cast<unsigned long long*>(&ctl->gsel[w]), ~bit);
       if (bfs_like) {
         atomic_or64(&ctl->bfs_bits[w], bit);
         atomicAnd(reinterpret_cast<unsigned long long*>(&ctl->sssp_bits[w]), ~bit);
+        atomicAnd(reinterpret_cast<unsigned long long*>(&ctl->ssel[w]), ~bit);
         atomic_or64(g.visited + static_cast<size_t>(r.source) * W + w, bit);
       } else {
         atomic_or64(&ctl->sssp_bits[w], bit);
+        atomic_or64(&ctl->ssel[w], bit);
         atomicAnd(reinterpret_cast<unsigned long long*>(&ctl->bfs_bits[w]), ~bit);
       }
       if (r.kind == 3 && r.k <= 0)
@@ -101,7 +106,12 @@ __global__ void k_admit(GroupDev g, DevGraph G, const AdmitReq* reqs, int n) {
   if (threadIdx.x == 0 && ctl->count[par] > 0) {
     ctl->done = 0;
     ctl->dir = decide_dir(ctl, ctl->count[par], ctl->edges[par], any_bits<W>(ctl->bfs_bits));
-    ctl->sdir = decide_sdir(ctl, ctl->edges[par], any_bits<W>(ctl->sssp_bits));
+    if (ctl->chunk_dir) {
+      ctl->sdir = any_bits<W>(ctl->gsel) ? kDirPull : kDirPush;
+      ctl->sscatter = any_bits<W>(ctl->ssel) ? 1 : 0;
+    } else {
+      split_sssp_slots<W>(ctl, decide_sdir(ctl, ctl->edges[par], any_bits<W>(ctl->sssp_bits)));
+    }
   }
 }
 
@@ -238,6 +248,7 @@ struct cgp_server {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   void loop();
+  int pick_slot();
   void finish_wcc(std::vector<uint64_t>& tickets);
   void retire(std::vector<int>& slots_to_retire, bool forced);
 };
@@ -326,6 +337,38 @@ void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
     ++completed;
   }
   done_cv.notify_all();
+}
+
+// A free slot for the next admission (mu held), or -1.  Slots are taken in
+// 32-slot cohorts, so that requests that arrive together share a chunk and
+// pass through their sparse and dense phases together (what the per-chunk
+// SSSP direction needs): first a chunk already taken by this admission pass,
+// then an empty chunk, then the chunk whose occupants were admitted last.
+int cgp_server::pick_slot() {
+  int best = -1;
+  long long best_key = -1;
+  for (int c0 = 0; c0 < S; c0 += 32) {
+    const int c1 = std::min(S, c0 + 32);
+    int free_slot = -1, occupied = 0, newest = -1;
+    bool this_pass = false;
+    for (int i = c0; i < c1; ++i) {
+      if (slot_ticket[i] < 0) {
+        if (free_slot < 0) free_slot = i;
+        continue;
+      }
+      ++occupied;
+      const int al = reqs[static_cast<uint64_t>(slot_ticket[i])].admit_level;
+      if (al < 0) this_pass = true;  // level set once the admission kernel ran
+      newest = std::max(newest, al);
+    }
+    if (free_slot < 0) continue;
+    const long long key = this_pass ? (3LL << 40) : occupied == 0 ? (2LL << 40) : newest;
+    if (key > best_key) {
+      best_key = key;
+      best = free_slot;
+    }
+  }
+  return best;
 }
 
 void cgp_server::retire(std::vector<int>& to_retire, bool forced) {
@@ -417,12 +460,7 @@ void cgp_server::loop() {
             wcc_tickets.push_back(tk);
             continue;
           }
-          int s = -1;
-          for (int i = 0; i < S; ++i)
-            if (slot_ticket[i] < 0) {
-              s = i;
-              break;
-            }
+          const int s = pick_slot();
           if (s < 0) break;
           pending.pop_front();
           slot_ticket[s] = static_cast<int64_t>(tk);
@@ -543,6 +581,7 @@ cgp_status cgp_server_create(cgp_graph* graph, int32_t slots, const cgp_options*
     sv->spec.has_bfs = true;
     sv->spec.has_sssp = true;
     sv->spec.uniform_inf = kServeInf;
+    sv->spec.serving = true;
     group_prepare(g, sv->ws.get(), sv->spec, sv->o, sv->stream);
     sv->slot_ticket.assign(S, -1);
     sv->admit_dev.ensure(kMaxWords * 64 * sizeof(AdmitReq));

@@ -110,9 +110,26 @@ typedef struct {
                                   <= 0: always scatter (push)                              */
   int32_t light_chunks;       /* SSSP gathers take light vertices in CTA chunks (groups of up
                                  to 256 slots): 0 = on, -1 = one warp per vertex           */
+  int32_t level_loop;         /* CGP_LOOP_*: how a traversal to convergence is driven     */
+  int32_t sssp_chunk_direction; /* SSSP gather/scatter decided per 32-slot chunk from the
+                                   chunk's own frontier (1), or for the whole group (-1);
+                                   0 = auto: per chunk in the serving loop, whole group in
+                                   batch runs                                              */
   int32_t reserved;
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
+
+/* level_loop values.  CHUNKS: CUDA graphs of levels_per_sync levels, the host
+ * reads the control block once per chunk (one chunk in flight).  DEVICE: one
+ * CUDA graph whose WHILE conditional node runs a level per iteration until
+ * the device-side done flag is set: the host waits once per traversal (it
+ * replaces the reference's per-level host synchronisation,
+ * frontier_engine.hxx:3044-3071).  AUTO is CHUNKS: kernels inside a graph
+ * with conditional nodes are invisible to kernel profilers, so the device
+ * loop is asked for explicitly. */
+#define CGP_LOOP_AUTO 0
+#define CGP_LOOP_CHUNKS 1
+#define CGP_LOOP_DEVICE 2
 
 /* Per-level record: iteration_profile_t (puercgp/include/puercgp/core/result.hxx:21-46). */
 typedef struct {

@@ -550,3 +550,111 @@ def test_sssp_gather_light_chunks(rmat_u32, nq, heavy):
                           layout="query")
         np.testing.assert_array_equal(r.values, ref)
 
+
+
+@pytest.mark.parametrize("loop", ["chunks", "device"])
+@pytest.mark.parametrize("per_sync", [0, 1, 3])
+def test_level_loop_forms_give_identical_results(rmat_u32, grid_f32, loop, per_sync):
+    """Host-checked graph chunks and the device-looped graph (WHILE node on
+    the done flag) give identical values on a shallow R-MAT and a deep grid,
+    and BFS runs take the same levels and push/pull split (SSSP level counts
+    may differ by a level between any two runs: relaxations within a level
+    see each other's writes)."""
+    for g, graph, kind in ((rmat_u32[0], rmat_u32[1], "bfs"), (rmat_u32[0], rmat_u32[1], "sssp"),
+                           (grid_f32[0], grid_f32[1], "sssp")):
+        src = g.pick_sources(70, seed=31)
+        descs = [cgp.QueryDescriptor(int(s), kind) for s in src]
+        r = cgp.run_batch(graph, descs, cgp.RunOptions(level_loop=loop, levels_per_sync=per_sync),
+                          layout="query")
+        ref, _ = oracle.batch(kind, g, src)
+        np.testing.assert_array_equal(r.values.view(ref.dtype), ref)
+        if kind == "bfs":
+            base = cgp.run_batch(graph, descs, cgp.RunOptions(use_cuda_graph=False),
+                                 layout="query")
+            assert (r.iterations, r.push_levels, r.pull_levels) == \
+                (base.iterations, base.push_levels, base.pull_levels)
+
+
+def test_device_loop_honours_max_iterations(rmat_u32):
+    g, graph = rmat_u32
+    src = g.pick_sources(8, seed=32)
+    r = cgp.run("bfs", graph, src, options=cgp.RunOptions(level_loop="device", max_iterations=2),
+                layout="query")
+    assert r.iterations == 2
+    ref, _ = oracle.batch("bfs", g, src)
+    v = r.values
+    # depths 0..2 are final after two levels; deeper vertices are still unreached
+    assert np.array_equal(np.where(ref <= 2, ref, INF), v)
+
+
+def _with_paths(g, paths, length, wkind):
+    """g plus `paths` disjoint paths of `length` vertices on new ids, with
+    fresh symmetric weights: sources on a path keep tiny frontiers."""
+    V = g.num_vertices
+    u = np.repeat(np.arange(V), np.diff(g.row_offsets))
+    keep = u < g.col_indices
+    src = [u[keep]]
+    dst = [g.col_indices[keep]]
+    for p in range(paths):
+        base = V + p * length
+        src.append(np.arange(base, base + length - 1))
+        dst.append(np.arange(base + 1, base + length))
+    h = cgp.csr_from_edges(V + paths * length, np.concatenate(src), np.concatenate(dst))
+    if wkind == "u32":
+        return h.with_weights("u32", 1, 64, seed=7)
+    return h.with_weights("f32", 1.0, 100.0, seed=7)
+
+
+def _split_component_sources(g, n_big, n_small, seed):
+    """n_big sources in the largest component, n_small outside it (vertices
+    with edges): their chunks' frontiers stay small while the others grow."""
+    lab = oracle.wcc_components(g).astype(np.int64)
+    big = np.bincount(lab).argmax()
+    deg = g.degrees()
+    a = g.pick_sources(n_big, seed=seed, allowed=(lab == big).astype(np.uint8))
+    b = g.pick_sources(n_small, seed=seed + 1, allowed=((lab != big) & (deg > 0)).astype(np.uint8))
+    return np.concatenate([a, b])
+
+
+@pytest.fixture(scope="module")
+def rmat_paths():
+    g = _with_paths(cgp.gen_rmat(12, 8, seed=101), 64, 40, "u32")
+    return g, cgp.CsrGraph(g)
+
+
+@pytest.fixture(scope="module")
+def grid_paths():
+    g = _with_paths(cgp.gen_grid(40, 50, 0.1, 0.01, seed=105), 32, 60, "f32")
+    return g, cgp.CsrGraph(g)
+
+
+@pytest.mark.parametrize("nq,kinds", [(64, "sssp"), (256, "sssp"), (200, "mixed"), (1024, "sssp")])
+@pytest.mark.parametrize("ratio", [0.02, 0.3])
+def test_sssp_direction_per_chunk(rmat_paths, nq, kinds, ratio):
+    """SSSP gather/scatter chosen per 32-slot chunk: chunks whose sources lie
+    on small path components keep scattering while the others gather in the
+    same level; results stay exact."""
+    g, graph = rmat_paths
+    src = _split_component_sources(g, nq // 2, nq - nq // 2, seed=nq)
+    if kinds == "mixed":
+        descs = [cgp.QueryDescriptor(int(s), "bfs" if i % 3 == 0 else "sssp")
+                 for i, s in enumerate(src)]
+    else:
+        descs = [cgp.QueryDescriptor(int(s), "sssp") for s in src]
+    opts = cgp.RunOptions(sssp_chunk_direction=1, sssp_pull_edge_ratio=ratio, mask_words=16)
+    r = cgp.run_batch(graph, descs, opts, layout="query")
+    for i, d in enumerate(descs):
+        exp = oracle.bfs(g, d.source).view(np.uint32) if d.kind == "bfs" else oracle.sssp(g, d.source)
+        np.testing.assert_array_equal(r.values[i].view(np.uint32), exp)
+
+
+def test_sssp_direction_per_chunk_f32_grid(grid_paths):
+    g, graph = grid_paths
+    src = _split_component_sources(g, 96, 32, seed=5)
+    descs = [cgp.QueryDescriptor(int(s), "sssp") for s in src]
+    for loop in ("chunks", "device"):
+        r = cgp.run_batch(graph, descs, cgp.RunOptions(sssp_chunk_direction=1,
+                                                       sssp_pull_edge_ratio=0.05,
+                                                       level_loop=loop), layout="query")
+        ref, _ = oracle.batch("sssp", g, src)
+        np.testing.assert_array_equal(r.values.view(np.float32), ref)
