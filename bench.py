@@ -575,6 +575,7 @@ def run_serve(args):
                     options=cgp.RunOptions(traversal_mode=args.mode,
                                            pull_edge_ratio=args.pull_edge_ratio,
                                            heavy_degree=args.heavy_degree,
+                                           sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
                                            sssp_chunk_direction=args.sssp_chunk_direction,
                                            profile_kernels=args.serve_profile)) as srv:
         poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
@@ -597,6 +598,7 @@ def run_serve(args):
             "offsets": "int64", "slots": st["slots"], "state_bytes": st["state_bytes"],
             "sssp_direction": {1: "per 32-slot chunk", -1: "per group"}.get(
                 args.sssp_chunk_direction, "auto (per 32-slot chunk)"),
+            "sssp_pull_edge_ratio": args.sssp_pull_edge_ratio,
             "seconds_per_rate": args.serve_seconds, "rates": rows, "graph_gen_s": gen_s}
     print(json.dumps(line), flush=True)
     if args.json_out:
@@ -774,7 +776,7 @@ def main():
 
     # ---- profiled step: per-kernel-class CUDA-event times + level counters
     kclass, level_trace = {}, {}
-    if not args.no_profile and args.workload in ("c1", "c2"):
+    if not args.no_profile and args.workload in ("c1", "c2", "c3"):
         for i, (d, o, (k, src)) in enumerate(zip(descs, opts, groups)):
             p = cgp.run_batch(graph, d, dataclasses.replace(o, profile_kernels=True,
                                                             profile_iterations=True),

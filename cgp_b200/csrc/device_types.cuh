@@ -141,6 +141,9 @@ struct GroupDev {
   uint64_t* planes;    // [K][V*W] depth bit planes
   uint32_t* values;    // [V*Qg] vertex-major values (SSSP, direct depths)
   uint64_t* hacc;      // [n_pheavy*W] pull accumulators of heavy vertices
+  uint64_t* fsum;      // [V] frontier summary: (level + 1) << 32 | 32-slot chunks with a
+                       // frontier bit, written for the frontier's vertices on levels that
+                       // screen sources by it (nullptr: not kept)
   int32_t* dense_list; // [V] SSSP frontier vertices with many active bits
   int32_t* hq_vertex;  // [n_heavy] heavy vertices of the current frontier
   int64_t* hq_start;   // [n_heavy] their first chunk in the level's chunk space

@@ -371,6 +371,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
   if (kt) kt->mark(kClassClear, s);
   k_clear_next<W><<<c, kBlock, 0, s>>>(L.g);
   ++n;
+  if (L.g.fsum != nullptr && (L.pull || L.spull)) {
+    k_frontier_summary<W><<<c, kBlock, 0, s>>>(L.g, L.G);
+    ++n;
+  }
   if (L.G.n_heavy) {
     k_heavy_queue<OT><<<c, kBlock, 0, s>>>(L.g, L.G);
     ++n;
@@ -546,6 +550,7 @@ GroupDev group_dev(Workspace* ws, const GroupSpec& spec, bool profiles) {
                  ? nullptr
                  : (spec.external_values ? spec.external_values : ws->values.as<uint32_t>());
   g.hacc = ws->hacc.as<uint64_t>();
+  g.fsum = ws->fsum.as<uint64_t>();
   g.dense_list = ws->dense.as<int32_t>();
   g.hq_vertex = ws->hq_vertex.as<int32_t>();
   g.hq_start = ws->hq_start.as<int64_t>();
@@ -590,6 +595,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
     moved |= ws->list1.ensure(static_cast<size_t>(V) * 4);
     moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
     moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8);
+    moved |= ws->fsum.ensure(static_cast<size_t>(V) * 8);
     moved |= ws->hq_vertex.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 4);
     moved |= ws->hq_start.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 8);
     if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
@@ -616,6 +622,7 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   ck(cudaMemsetAsync(ws->stamp.p, 0xff, static_cast<size_t>(V) * 4, s), "memset stamp");
   ck(cudaMemsetAsync(ws->hacc.p, 0, static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8, s),
      "memset hacc");
+  ck(cudaMemsetAsync(ws->fsum.p, 0, static_cast<size_t>(V) * 8, s), "memset fsum");
   if (spec.depth_mode == kDepthPlanes)
     ck(cudaMemsetAsync(ws->planes.p, 0, static_cast<size_t>(kInitialPlanes) * mask_bytes, s),
        "memset planes");

@@ -116,6 +116,7 @@ struct KernelTimer {
 struct Workspace {
   int device = 0;
   DevBuf visited, fbuf0, fbuf1, list0, list1, stamp, planes, values, hacc, dense, hq_vertex, hq_start;
+  DevBuf fsum;  // frontier summary words (uint64 per vertex)
   DevBuf ctl, prof, slots, stage, wcc, qmap;
   LevelCtl* hctl = nullptr;  // pinned, 2 snapshots
   dev::SlotDev* hslots = nullptr;  // pinned, kMaxWords*64 entries

@@ -155,6 +155,27 @@ __device__ __forceinline__ int jth_set_bit(const uint64_t* bits, int j) {
   return -1;
 }
 
+// Bit c: 32-slot chunk c of the mask has a bit set.
+template <int W>
+__device__ __forceinline__ uint32_t chunk_bits(const uint64_t (&m)[W]) {
+  uint32_t c = 0;
+#pragma unroll
+  for (int i = 0; i < W; ++i) {
+    c |= (static_cast<uint32_t>(m[i]) != 0u ? 1u : 0u) << (2 * i);
+    c |= (static_cast<uint32_t>(m[i] >> 32) != 0u ? 1u : 0u) << (2 * i + 1);
+  }
+  return c;
+}
+
+// Frontier summary of vertex u at `level`: its 32-slot chunks with a frontier
+// bit, when the summary was written for this level (a stale word reads as
+// "no chunk").  Only ever used to skip mask and row loads: a vertex of the
+// current frontier always has its word, so no frontier bit is missed.
+__device__ __forceinline__ uint32_t summary_chunks(const uint64_t* fsum, int level, int32_t u) {
+  const uint64_t x = fsum[u];
+  return (x >> 32) == static_cast<uint64_t>(level + 1) ? static_cast<uint32_t>(x) : 0u;
+}
+
 // Pointers of the current level.
 struct LevelView {
   int level;
@@ -553,6 +574,15 @@ __device__ __forceinline__ void pull_commit(const GroupDev& g, int64_t V,
   g.stamp[v] = lv.level + 1;
 }
 
+// A pull level whose frontier holds fewer than 1/16 of the vertices screens
+// in-edges by the frontier summary: a source outside the frontier costs an
+// 8-byte word that stays in L2 instead of its W-word mask.
+__device__ __forceinline__ bool bfs_pull_uses_summary(const GroupDev& g, const LevelCtl* ctl,
+                                                      const LevelView& lv, int64_t V) {
+  return g.fsum != nullptr && ctl->dir == kDirPull &&
+         16ULL * ctl->count[lv.par] < static_cast<unsigned long long>(V);
+}
+
 // Pull level (bottom-up): every non-heavy vertex with unvisited active bits
 // ORs the current-frontier masks of its in-neighbours until every needed bit
 // is found (early exit).  Reads only the current frontier, so depths are
@@ -570,6 +600,7 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
   const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
   const unsigned long long V = static_cast<unsigned long long>(G.V);
+  const bool use_sum = bfs_pull_uses_summary(g, ctl, lv, G.V);
   uint64_t uni[W];
 #pragma unroll
   for (int i = 0; i < W; ++i) uni[i] = 0;
@@ -599,12 +630,18 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
     const bool work = valid && !heavy && deg > 0 && mask_any<W>(need);
     pverts += work ? 1 : 0;
     if (work && deg <= 32) {
+      const uint32_t nch = chunk_bits<W>(need);
       // four in-edges per step: their column and mask loads are independent
       // and stay in flight together; early exit is checked once per step
       for (int64_t e = beg; e < end; e += 4) {
         int32_t us[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) us[j] = (e + j < end) ? G.pcol[e + j] : -1;
+        if (use_sum) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (us[j] >= 0 && !(summary_chunks(g.fsum, lv.level, us[j]) & nch)) us[j] = -1;
+        }
         pedges += static_cast<unsigned long long>(end - e < 4 ? end - e : 4);
         bool full = true;
 #pragma unroll
@@ -632,14 +669,18 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
         bn[i] = __shfl_sync(kFull, need[i], src);
         a[i] = 0;
       }
+      const uint32_t bch = chunk_bits<W>(bn);
       for (int64_t e0 = bb; e0 < be; e0 += 32) {
         const int64_t e = e0 + lane;
         if (e < be) {
           ++pedges;
-          uint64_t fu[W];
-          load_mask<W>(lv.fcur + static_cast<size_t>(G.pcol[e]) * W, fu);
+          const int32_t u = G.pcol[e];
+          if (!use_sum || (summary_chunks(g.fsum, lv.level, u) & bch)) {
+            uint64_t fu[W];
+            load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, fu);
 #pragma unroll
-          for (int i = 0; i < W; ++i) a[i] |= fu[i] & bn[i];
+            for (int i = 0; i < W; ++i) a[i] |= fu[i] & bn[i];
+          }
         }
         warp_or_reduce<W>(a);
         bool full = true;
@@ -718,9 +759,13 @@ __global__ void __launch_bounds__(kBlock) k_bfs_pull_heavy(GroupDev g, DevGraph 
 #pragma unroll
     for (int i = 0; i < W; ++i) a[i] = 0;
     if (threadIdx.x == 0) atomicAdd(&g.ctl->lc.pull_edges, static_cast<unsigned long long>(ce - cb));
+    const bool use_sum = bfs_pull_uses_summary(g, ctl, lv, G.V);
+    const uint32_t nch = chunk_bits<W>(need);
     for (int64_t e = cb + threadIdx.x; e < ce; e += blockDim.x) {
+      const int32_t u = G.pcol[e];
+      if (use_sum && !(summary_chunks(g.fsum, lv.level, u) & nch)) continue;
       uint64_t fu[W];
-      load_mask<W>(lv.fcur + static_cast<size_t>(G.pcol[e]) * W, fu);
+      load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, fu);
 #pragma unroll
       for (int i = 0; i < W; ++i) a[i] |= fu[i] & need[i];
     }
@@ -1596,16 +1641,35 @@ __device__ __forceinline__ int gather_screen_qs(const LevelCtl* ctl, const Level
   return qs;
 }
 
-// Bit c: 32-slot chunk c of the mask has a bit set.
+// 32-slot chunks that hold a gathering SSSP slot at this level.
 template <int W>
-__device__ __forceinline__ uint32_t chunk_bits(const uint64_t (&m)[W]) {
-  uint32_t c = 0;
+__device__ __forceinline__ uint32_t gather_chunks(const LevelCtl* ctl) {
+  uint64_t gs[W];
 #pragma unroll
-  for (int i = 0; i < W; ++i) {
-    c |= (static_cast<uint32_t>(m[i]) != 0u ? 1u : 0u) << (2 * i);
-    c |= (static_cast<uint32_t>(m[i] >> 32) != 0u ? 1u : 0u) << (2 * i + 1);
+  for (int i = 0; i < W; ++i) gs[i] = ctl->gsel[i];
+  return chunk_bits<W>(gs);
+}
+
+// Writes the frontier summary of the current frontier's vertices on levels
+// that screen sources by it (screened SSSP gathers, sparse BFS pulls); other
+// levels return at once.  Words of vertices outside the frontier keep an older
+// level's stamp and read as empty.
+template <int W>
+__global__ void __launch_bounds__(kBlock) k_frontier_summary(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done) return;
+  const LevelView lv = level_view(g);
+  const bool sssp = ctl->sdir == kDirPull && gather_screen_qs<W>(ctl, lv, G.E) < 0;
+  if (!sssp && !bfs_pull_uses_summary(g, ctl, lv, G.V)) return;
+  const unsigned long long n = ctl->count[lv.par];
+  const uint64_t stamp = static_cast<uint64_t>(lv.level + 1) << 32;
+  for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+       i < n; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+    const int32_t v = lv.list[i];
+    uint64_t m[W];
+    load_mask<W>(lv.fcur + static_cast<size_t>(v) * W, m);
+    g.fsum[v] = stamp | chunk_bits<W>(m);
   }
-  return c;
 }
 
 // Whether the lane reads part r of a source row whose 32-slot chunk bits are
@@ -1625,7 +1689,8 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
                                                  int lane, int4* stage,
                                                  uint32_t (&best)[GatherVec<W>::kSlots],
                                                  unsigned long long& pairs,
-                                                 unsigned& scanned, int screen_qs) {
+                                                 unsigned& scanned, int screen_qs,
+                                                 uint32_t gch) {
   using GV = GatherVec<W>;
   constexpr int E = GV::kElem;
   constexpr int P = GV::kParts;
@@ -1641,9 +1706,14 @@ __device__ __forceinline__ void gather_edges_vec(const GroupDev& g, const DevGra
     if (e < ee) {
       u = G.pcol[e];
       wb = weight_bits<WK>(G.pw, e);
-      if (screen_qs < 0) {
-        // sparse frontier: skip in-edges whose source has no SSSP frontier
-        // bit, and the source row's 32-slot chunks that have none
+      if (screen_qs < 0 && g.fsum != nullptr) {
+        // sparse frontier: skip in-edges whose source has no gathering
+        // frontier chunk, and the source row's chunks without one, by the
+        // frontier summary (pairs are counted per 32-slot chunk)
+        cm = summary_chunks(g.fsum, lv.level, u) & gch;
+        k = __popc(cm) << 5;
+      } else if (screen_qs < 0) {
+        // the same from the source's W-word mask
         uint64_t m[W];
         load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
         // the next batch's source masks move to L2 while this batch's rows load
@@ -1740,6 +1810,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   int32_t pend_v = 0;  // lane i: i-th vertex waiting to be appended
   int pend_n = 0;      // uniform
   const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const uint32_t gch = gather_chunks<W>(ctl);
   const unsigned long long V = static_cast<unsigned long long>(G.V);
   // the next vertex's offsets are loaded while the current one is gathered
   int64_t nbeg = 0, nend = 0;
@@ -1768,7 +1839,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
       }
     }
     gather_edges_vec<W, WK>(g, G, lv, sb, pmask, beg, end, lane, s_stage[wib], best, pairs,
-                            scanned, screen_qs);
+                            scanned, screen_qs, gch);
     // commit (the warp owns v's row this level: the row read above is current)
     uint32_t imp = 0;
 #pragma unroll
@@ -1859,6 +1930,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
   uint32_t pmask, smask;
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const uint32_t gch = gather_chunks<W>(ctl);
   const size_t Qg = static_cast<size_t>(g.Qg);
   const uint32_t* lanebase = g.values + lane * E;
   WarpAppender ap;
@@ -1927,7 +1999,10 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
         const int64_t e = s_beg[k] + (f - s_pre[k]);
         u = G.pcol[e];
         wb = weight_bits<WK>(G.pw, e);
-        if (screen_qs < 0) {
+        if (screen_qs < 0 && g.fsum != nullptr) {
+          cm = summary_chunks(g.fsum, lv.level, u) & gch;
+          cnt = __popc(cm) << 5;
+        } else if (screen_qs < 0) {
           uint64_t m[W];
           load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
           // the next batch's source masks move to L2 while this batch's rows load
@@ -2077,6 +2152,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
   const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const uint32_t gch = gather_chunks<W>(ctl);
   if ((kMode == 1 && screen_qs < 0) || (kMode == 2 && screen_qs >= 0)) return;
   const size_t Qg = static_cast<size_t>(g.Qg);
   uint64_t uni[W];
@@ -2110,7 +2186,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) best[j] = 0xffffffffu;
     gather_edges_vec<W, WK, kMode == 2>(g, G, lv, sb, pmask, wb, we, lane, s_stage[wib], best,
-                                        pairs, scanned, screen_qs);
+                                        pairs, scanned, screen_qs, gch);
 #pragma unroll
     for (int j = 0; j < GV::kSlots; ++j) {
       const int q = (32 * (j / E) + lane) * E + (j % E);

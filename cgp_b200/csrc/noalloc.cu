@@ -175,6 +175,7 @@ extern "C" cgp_status cgp_bfs_batch_noalloc(const void* row_offsets, int32_t off
     g.planes = nullptr;
     g.values = reinterpret_cast<uint32_t*>(out);
     g.hacc = nullptr;
+    g.fsum = nullptr;
     g.dense_list = nullptr;
     g.prof = nullptr;
     g.Qg = nq;

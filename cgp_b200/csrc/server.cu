@@ -296,6 +296,7 @@ GroupDev server_dev(cgp_server* sv) {
   g.planes = nullptr;
   g.values = ws->values.as<uint32_t>();
   g.hacc = ws->hacc.as<uint64_t>();
+  g.fsum = ws->fsum.as<uint64_t>();
   g.dense_list = ws->dense.as<int32_t>();
   g.hq_vertex = nullptr;
   g.hq_start = nullptr;
