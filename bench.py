@@ -588,6 +588,9 @@ def run_serve(args):
             row["retire_ms"] = s1["retire_ms"] - s0["retire_ms"]
             row["retire_passes"] = s1["retire_passes"] - s0["retire_passes"]
             row["admit_ms"] = s1["admit_ms"] - s0["admit_ms"]
+            sc = s1["sssp_chunk_levels"] - s0["sssp_chunk_levels"]
+            row["gathering_chunk_frac"] = ((s1["gather_chunk_levels"] - s0["gather_chunk_levels"])
+                                           / sc if sc else None)
             if args.serve_profile:
                 row["kernel_ms"] = {k: s1["kernel_ms"].get(k, 0) - s0["kernel_ms"].get(k, 0)
                                     for k in s1["kernel_ms"]}

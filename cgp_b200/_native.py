@@ -40,7 +40,7 @@ class CgpOptions(Structure):
         ("depth_mode", c_int32), ("heavy_degree", c_int32), ("max_queries", c_int32),
         ("discard_results", c_int32), ("profile_kernels", c_int32), ("dense_unroll", c_int32),
         ("sssp_pull_edge_ratio", c_double), ("light_chunks", c_int32), ("level_loop", c_int32),
-        ("sssp_chunk_direction", c_int32), ("reserved", c_int32), ("stream", c_void_p),
+        ("sssp_chunk_direction", c_int32), ("bfs_pull_form", c_int32), ("stream", c_void_p),
     ]
 
 
@@ -89,7 +89,8 @@ class CgpServerStats(Structure):
     _fields_ = [("slots", c_int32), ("active_slots", c_int32), ("queued", c_int64),
                 ("completed", c_int64), ("levels", c_int64), ("busy_ms", c_double),
                 ("state_bytes", c_int64), ("admit_ms", c_double), ("retire_ms", c_double),
-                ("retire_passes", c_int64), ("kernel_ms", c_double * 12)]
+                ("retire_passes", c_int64), ("kernel_ms", c_double * 12),
+                ("sssp_chunk_levels", c_int64), ("gather_chunk_levels", c_int64)]
 
 
 # name -> (restype, argtypes)

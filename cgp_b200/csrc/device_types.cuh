@@ -57,6 +57,9 @@ struct LevelCounters {
   unsigned long long improved;
   unsigned long long spull_vertices;
   unsigned long long spull_edges;
+  unsigned long long live_chunks;  // sum over frontier vertices of out-degree x gathering
+                                   // chunks with a frontier bit (row chunks a screened
+                                   // gather reads)
 };
 
 // Control block of one traversal group (device memory).
@@ -74,6 +77,8 @@ struct LevelCtl {
   uint64_t ssel[kMaxW];         // SSSP slots that scatter (push) at the current level
   unsigned long long cedges[2 * kMaxW];  // per 32-slot chunk: out-edges of the next
                                          // frontier's vertices with an SSSP bit in it
+  unsigned long long sssp_chunk_levels;    // sum over levels of chunks with SSSP slots
+  unsigned long long gather_chunk_levels;  // ... and of those that gathered
   int32_t sscatter;             // ssel has a bit: the scatter kernels have work
   int32_t chunk_dir;            // SSSP direction decided per 32-slot chunk
   int32_t level;
@@ -96,6 +101,9 @@ struct LevelCtl {
   unsigned long long dense_count;  // SSSP vertices queued for the dense kernel this level
   unsigned long long hq_packed;    // heavy frontier queue: count << 40 | chunks, this level
   unsigned long long prev_improved; // SSSP entries improved by the previous level
+  unsigned long long prev_pull_edges; // in-edges the previous BFS pull level read
+  int32_t prev_dir;                 // BFS direction of the previous level
+  int32_t bfs_chunked;              // the BFS pull may run in CTA chunks (chunk table built)
   LevelCounters lc;                // counters of the current level
   LevelCounters total;             // sums over all levels
 };

@@ -332,10 +332,11 @@ struct Grids {
   int gather_heavy_vec;
   int gather_chunked;
   int gather_heavy_vec2;
+  int bfs_chunked;
 };
 
 struct LevelLaunch {
-  GroupDev g;
+  GroupDev g{};
   DevGraph G;
   Grids gr;
   bool has_bfs;
@@ -346,6 +347,8 @@ struct LevelLaunch {
   bool lchunks;      // light vertices gathered in CTA chunks (W <= 4)
   int dense_unroll;  // edges per step of the dense SSSP kernel (1 or 2)
   KernelTimer* kt;   // per-class event timing (non-graph runs only)
+  bool heavy_push = false;                // heavy-queue push kernels are part of a level
+  bool bfs_chunked = false;               // chunked light-vertex BFS pull is part of a pull level
   bool chunk_dir = false;                 // census of per-chunk frontier edges
   bool device_loop = false;               // level end sets a WHILE node's condition
   cudaGraphConditionalHandle loop = 0;    // ... this one
@@ -369,13 +372,13 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
   KernelTimer* kt = L.kt;
   int n = 0;
   if (kt) kt->mark(kClassClear, s);
-  k_clear_next<W><<<c, kBlock, 0, s>>>(L.g);
+  k_clear_next<W><<<c, kBlock, 0, s>>>(L.g, L.G.E);
   ++n;
   if (L.g.fsum != nullptr && (L.pull || L.spull)) {
-    k_frontier_summary<W><<<c, kBlock, 0, s>>>(L.g, L.G);
+    k_frontier_summary<W, OT><<<c, kBlock, 0, s>>>(L.g, L.G);
     ++n;
   }
-  if (L.G.n_heavy) {
+  if (L.heavy_push) {
     k_heavy_queue<OT><<<c, kBlock, 0, s>>>(L.g, L.G);
     ++n;
   }
@@ -383,7 +386,7 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
     if (kt) kt->mark(kClassBfsPush, s);
     k_bfs_push<W, OT, DEPTH><<<t, kBlock, 0, s>>>(L.g, L.G);
     ++n;
-    if (L.G.n_heavy) {
+    if (L.heavy_push) {
       k_bfs_push_heavy<W, OT, DEPTH><<<h, kBlock, 0, s>>>(L.g, L.G);
       ++n;
     }
@@ -391,6 +394,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
       if (kt) kt->mark(kClassBfsPull, s);
       k_bfs_pull<W, OT, DEPTH><<<t, kBlock, 0, s>>>(L.g, L.G);
       ++n;
+      if (L.bfs_chunked) {  // each of the two forms returns at once on the other's levels
+        k_bfs_pull_chunked<W, OT, DEPTH><<<L.gr.bfs_chunked, kBlock, 0, s>>>(L.g, L.G);
+        ++n;
+      }
       if (L.G.n_pheavy) {
         k_bfs_pull_heavy<W, OT><<<h, kBlock, 0, s>>>(L.g, L.G);
         k_bfs_pull_heavy_commit<W, OT, DEPTH><<<std::max(1, (L.G.n_pheavy + kBlock - 1) / kBlock), kBlock, 0, s>>>(L.g, L.G);
@@ -407,7 +414,7 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
     else
       k_sssp_dense<W, OT, WK, 1><<<L.gr.dense, kBlock, 0, s>>>(L.g, L.G);
     n += 2;
-    if (L.G.n_heavy) {
+    if (L.heavy_push) {
       if (kt) kt->mark(kClassSsspHeavy, s);
       k_sssp_push_heavy<W, OT, WK><<<h, kBlock, 0, s>>>(L.g, L.G);
       ++n;
@@ -462,7 +469,9 @@ template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
   static int tile = 0, heavy = 0, dense = 0, dense2 = 0, gather = 0, gather_heavy = 0;
   static int gather_vec = 0, gather_heavy_vec = 0, gather_chunked = 0, gather_heavy_vec2 = 0;
+  static int bfs_chunked = 0;
   if (tile == 0) {
+    bfs_chunked = occupancy_grid(k_bfs_pull_chunked<W, OT, DEPTH>, sms);
     if constexpr (W <= 4) gather_chunked = occupancy_grid(k_sssp_pull_chunked<W, OT, WK>, sms);
     gather_vec = occupancy_grid(k_sssp_pull_vec<W, OT, WK>, sms);
     gather_heavy_vec = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK, (W <= 4 ? 1 : 0)>, sms);
@@ -490,6 +499,7 @@ Grids grids_t(int sms) {
   g.gather_heavy_vec = gather_heavy_vec;
   g.gather_chunked = gather_chunked;
   g.gather_heavy_vec2 = gather_heavy_vec2;
+  g.bfs_chunked = bfs_chunked;
   return g;
 }
 
@@ -538,7 +548,7 @@ Dispatch dispatch(int W, int ob, int depth, int wk) {
 }
 
 GroupDev group_dev(Workspace* ws, const GroupSpec& spec, bool profiles) {
-  GroupDev g;
+  GroupDev g{};
   g.visited = ws->visited.as<uint64_t>();
   g.fbuf0 = ws->fbuf0.as<uint64_t>();
   g.fbuf1 = ws->fbuf1.as<uint64_t>();
@@ -596,8 +606,10 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
     moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
     moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8);
     moved |= ws->fsum.ensure(static_cast<size_t>(V) * 8);
-    moved |= ws->hq_vertex.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 4);
-    moved |= ws->hq_start.ensure(static_cast<size_t>(std::max(1, hp.heavy.n)) * 8);
+    // heavy-queue capacity: every heavy vertex, or a whole small frontier
+    const size_t hq_cap = std::max<size_t>(std::max(1, hp.heavy.n), kSmallFrontier);
+    moved |= ws->hq_vertex.ensure(hq_cap * 4);
+    moved |= ws->hq_start.ensure(hq_cap * 8);
     if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
     if (spec.depth_mode == kDepthPlanes) {
       moved |= ws->planes.ensure(static_cast<size_t>(kInitialPlanes) * mask_bytes);
@@ -655,6 +667,8 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
       std::max(1.0, o.pull_edge_ratio * static_cast<double>(g->E)));
   c.sssp_gather = sssp_gather_on(g, o) ? 1 : 0;
   c.chunk_dir = sssp_chunk_dir(spec, o) ? 1 : 0;
+  c.bfs_chunked = (spec.has_bfs && o.bfs_pull_form >= 0 && hp.plight.chunks > 0) ? 1 : 0;
+  c.prev_dir = kDirPush;
   c.sssp_pull_edge_threshold = static_cast<unsigned long long>(
       std::max(1.0, o.sssp_pull_edge_ratio * static_cast<double>(g->E)));
   ck(cudaMemcpyAsync(ws->ctl.p, &c, sizeof(LevelCtl), cudaMemcpyHostToDevice, s), "upload ctl");
@@ -692,6 +706,8 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   int mode = o.traversal_mode;
   if (!g->can_gather()) mode = CGP_MODE_PUSH;
   L.pull = mode != CGP_MODE_PUSH;
+  L.heavy_push = L.G.n_heavy > 0 || g->max_degree > 32;
+  L.bfs_chunked = L.pull && spec.has_bfs && L.G.n_plight_chunks > 0 && o.bfs_pull_form >= 0;
   L.spull = spec.has_sssp && sssp_gather_on(g, o);
   {
     // vector gather: kElem-slot vectors must stay inside rows and be aligned
@@ -715,7 +731,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
                              (spec.has_bfs ? 1 : 0) | (spec.has_sssp ? 2 : 0) | (L.pull ? 4 : 0) |
                                  (o.profile_iterations ? 8 : 0) | (L.dense_unroll == 2 ? 16 : 0) |
                                  (L.spull ? 32 : 0) | (L.lchunks ? 64 : 0) | (loop ? 128 : 0) |
-                                 (L.chunk_dir ? 256 : 0),
+                                 (L.chunk_dir ? 256 : 0) | (L.bfs_chunked ? 512 : 0),
                              levels, spec.Qg, static_cast<int>(L.G.heavy_degree), ws->generation,
                              reinterpret_cast<uint64_t>(L.g.values));
   auto it = ws->graphs.find(key);
@@ -960,8 +976,10 @@ cgp_status cgp_graph_create(const void* row_offsets, int32_t offset_bytes,
     }
     if (hrow[0] != 0 || hrow[num_vertices] != num_edges)
       throw ApiError{CGP_ERR_INVALID_ARG, "row_offsets must start at 0 and end at num_edges"};
-    for (int64_t v = 0; v < num_vertices; ++v)
+    for (int64_t v = 0; v < num_vertices; ++v) {
       if (hrow[v + 1] < hrow[v]) throw ApiError{CGP_ERR_INVALID_ARG, "row_offsets not monotone"};
+      G.max_degree = std::max(G.max_degree, hrow[v + 1] - hrow[v]);
+    }
     std::vector<int32_t> hcol(num_edges);
     if (num_edges > 0)
       ck(cudaMemcpy(hcol.data(), col_indices, num_edges * 4, kind), "read columns");

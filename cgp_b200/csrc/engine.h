@@ -137,6 +137,7 @@ struct GraphImpl {
   int device = 0;
   int num_sms = 148;
   int64_t V = 0, E = 0;
+  int64_t max_degree = 0;  // largest out-degree of the traversal CSR
   int offset_bytes = 4;
   int weight_kind = CGP_WEIGHT_NONE;
   bool symmetric = false;

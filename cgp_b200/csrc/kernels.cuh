@@ -203,6 +203,20 @@ __device__ __forceinline__ LevelView level_view(const GroupDev& g) {
   return lv;
 }
 
+// Frontier vertices that a push level's tile kernels expand themselves: out-
+// degree at most the returned limit.  Larger lists go to the heavy queue as
+// kHeavyChunk-edge CTA work items: lists above heavy_degree always, and on a
+// small frontier (<= kSmallFrontier vertices, e.g. the sources' level) every
+// list above 32 edges, so that a few long lists are not each walked by a
+// single warp while most warps of the grid have nothing to do.
+constexpr unsigned long long kSmallFrontier = 4096;
+
+__device__ __forceinline__ int64_t push_light_limit(const GroupDev& g, const DevGraph& G,
+                                                    unsigned long long count) {
+  return (g.hq_vertex != nullptr && count <= kSmallFrontier && G.heavy_degree > 32)
+             ? 32 : G.heavy_degree;
+}
+
 // ------------------------------------------------------- depth recording
 // Records depth `depth_abs` (level + 1) for the newly visited bits `nw` of
 // vertex n: direct mode writes values[n][q] = depth_abs - base[q]; planes
@@ -345,6 +359,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
   const LevelView lv = level_view(g);
   WarpAppender ap;
   const unsigned long long n = ctl->count[lv.par];
+  const int64_t light = push_light_limit(g, G, n);
   uint64_t sel[W];
 #pragma unroll
   for (int i = 0; i < W; ++i) sel[i] = ctl->bfs_bits[i] & ctl->expand[i];
@@ -378,7 +393,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
       for (int i = 0; i < W; ++i) f[i] &= sel[i];
     }
     const int64_t deg = end - beg;
-    const bool work = valid && mask_any<W>(f) && deg > 0 && deg <= G.heavy_degree;
+    const bool work = valid && mask_any<W>(f) && deg > 0 && deg <= light;
 
     unsigned big = __ballot_sync(kFull, work && deg > 32);
     while (big) {
@@ -458,11 +473,12 @@ __global__ void __launch_bounds__(kBlock) k_heavy_queue(GroupDev g, DevGraph G) 
   if (ctl->done || (ctl->dir != kDirPush && !ctl->sscatter)) return;
   const LevelView lv = level_view(g);
   const unsigned long long n = ctl->count[lv.par];
+  const int64_t light = push_light_limit(g, G, n);
   for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
        i < n; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
     const int32_t u = lv.list[i];
     const int64_t deg = row_at<OT>(G.row, static_cast<int64_t>(u) + 1) - row_at<OT>(G.row, u);
-    if (deg <= G.heavy_degree) continue;
+    if (deg <= light) continue;
     const unsigned long long chunks = static_cast<unsigned long long>((deg + kHeavyChunk - 1) / kHeavyChunk);
     const unsigned long long old = atomicAdd(&ctl->hq_packed, (1ULL << kQueueShift) | chunks);
     const unsigned long long slot = old >> kQueueShift;
@@ -531,13 +547,28 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push_heavy(GroupDev g, DevGraph 
   warp_add(pairs, &g.ctl->lc.new_pairs, lane);
 }
 
+// Which light-vertex pull form a BFS pull level uses.  The chunked form
+// (k_bfs_pull_chunked) keeps 32 in-edges in flight per warp but checks early
+// exit once per 32-edge batch; the lane-per-vertex form (k_bfs_pull) stops a
+// vertex after the first in-edges that cover its needed bits.  The chunked
+// form runs where few vertices stop early: the first pull level after push
+// levels (bits are still rare, almost every in-edge is read) and levels after
+// a pull level that read at least half of the in-edges.
+__device__ __forceinline__ bool bfs_pull_chunked_level(const LevelCtl* ctl, int64_t E) {
+  if (!ctl->bfs_chunked) return false;
+  return ctl->prev_dir != kDirPull || 2 * ctl->prev_pull_edges >= static_cast<unsigned long long>(E);
+}
+
 // Zeroes the next-frontier buffer where the previous frontier left bits
 // (exactly the vertices of that frontier's list).  Push levels only: a pull
 // level rewrites every vertex's next mask.
 template <int W>
-__global__ void __launch_bounds__(kBlock) k_clear_next(GroupDev g) {
+__global__ void __launch_bounds__(kBlock) k_clear_next(GroupDev g, int64_t E) {
   const LevelCtl* ctl = g.ctl;
-  if (ctl->done || ctl->dir != kDirPush) return;
+  if (ctl->done) return;
+  // a lane-per-vertex pull level rewrites every vertex's next mask; the
+  // chunked one writes only vertices with new bits
+  if (ctl->dir != kDirPush && !bfs_pull_chunked_level(ctl, E)) return;
   const LevelView lv = level_view(g);
   const unsigned long long n = ctl->prev_count;
   const int32_t* plist = lv.nlist;  // list of the previous frontier
@@ -591,6 +622,7 @@ template <int W, typename OT, int DEPTH>
 __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->dir != kDirPull) return;
+  if (G.n_plight_chunks > 0 && bfs_pull_chunked_level(ctl, G.E)) return;
   const LevelView lv = level_view(g);
   uint64_t act[W];
 #pragma unroll
@@ -703,6 +735,153 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
     }
     warp_append(app, v, static_cast<uint64_t>(deg), lv.nlist, lv.ncount, lv.nedges, lane);
   }
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(pairs, &g.ctl->lc.new_pairs, lane);
+  warp_add(pverts, &g.ctl->lc.pull_vertices, lane);
+  warp_add(pedges, &g.ctl->lc.pull_edges, lane);
+}
+
+// Pull level (bottom-up), light vertices in CTA chunks of the pull CSR's light
+// chunk table (<= kLightChunkVerts vertices, <= kLightChunkEdges in-edges):
+// the CTA's warps split the chunk's in-edges evenly across vertex boundaries,
+// each lane loads one in-edge's source frontier mask and ORs its needed bits
+// into the vertex's accumulator in shared memory; before a batch a lane skips
+// its in-edge once the vertex's accumulator covers its need (early exit per
+// 32-edge batch).  After a barrier each vertex is committed once: next-frontier
+// words (cleared beforehand by k_clear_next), visited, depth, stamp, append.
+// Reads only the current frontier, so depths stay exactly level-synchronous.
+template <int W, typename OT, int DEPTH>
+__global__ void __launch_bounds__(kBlock) k_bfs_pull_chunked(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPull || G.n_plight_chunks == 0 ||
+      !bfs_pull_chunked_level(ctl, G.E))
+    return;
+  const LevelView lv = level_view(g);
+  __shared__ int32_t s_v[kLightChunkVerts];
+  __shared__ int64_t s_beg[kLightChunkVerts];
+  __shared__ int32_t s_pre[kLightChunkVerts + 1];
+  __shared__ unsigned long long s_need[kLightChunkVerts][W];
+  __shared__ unsigned long long s_acc[kLightChunkVerts][W];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  uint64_t act[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i)
+    act[i] = ctl->active[lv.par][i] & ctl->bfs_bits[i] & ctl->expand[i];
+  const bool use_sum = bfs_pull_uses_summary(g, ctl, lv, G.V);
+  WarpAppender ap;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long pairs = 0, pverts = 0, pedges = 0;
+  for (int c = blockIdx.x; c < G.n_plight_chunks; c += gridDim.x) {
+    const int cs = G.plight_chunk_start[c];
+    const int nv = G.plight_chunk_start[c + 1] - cs;
+    if (wib == 0) {
+      int32_t v = 0;
+      int64_t b = 0;
+      int d = 0;
+      if (lane < nv) {
+        v = G.plight[cs + lane];
+        b = row_at<OT>(G.prow, v);
+        uint64_t vis[W];
+        load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+          const uint64_t nd = ~vis[i] & act[i];
+          s_need[lane][i] = nd;
+          s_acc[lane][i] = 0;
+          any |= nd != 0;
+        }
+        // a vertex that needs nothing contributes no in-edges to the walk
+        d = any ? static_cast<int>(row_at<OT>(G.prow, static_cast<int64_t>(v) + 1) - b) : 0;
+        pverts += any ? 1 : 0;
+      }
+      int inc = d;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += t;
+      }
+      if (lane < nv) {
+        s_v[lane] = v;
+        s_beg[lane] = b;
+        s_pre[lane + 1] = inc;
+      }
+      if (lane == 0) s_pre[0] = 0;
+    }
+    __syncthreads();
+    const int total = s_pre[nv];
+    const int seg = (total + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const int fa = min(total, wib * seg);
+    const int fb = min(total, fa + seg);
+    for (int f0 = fa; f0 < fb; f0 += 32) {
+      const int f = f0 + lane;
+      if (f < fb) {
+        int lo = 0, hi = nv - 1;  // owner: last k with s_pre[k] <= f
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_pre[mid] <= f) lo = mid;
+          else hi = mid - 1;
+        }
+        const int k = lo;
+        uint64_t nd[W];
+        bool open = false;
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+          nd[i] = s_need[k][i];
+          open |= (s_acc[k][i] & nd[i]) != nd[i];
+        }
+        if (open) {
+          ++pedges;
+          const int32_t u = G.pcol[s_beg[k] + (f - s_pre[k])];
+          if (!use_sum || (summary_chunks(g.fsum, lv.level, u) & chunk_bits<W>(nd))) {
+            uint64_t fu[W];
+            load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, fu);
+#pragma unroll
+            for (int i = 0; i < W; ++i) {
+              const uint64_t x = fu[i] & nd[i];
+              if (x) atomicOr(&s_acc[k][i], static_cast<unsigned long long>(x));
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // commit: warp wib takes vertices wib, wib + 8, ... (lane 0 of the warp)
+    for (int k = wib; k < nv; k += kWarpsPerBlock) {
+      bool app = false;
+      const int32_t v = s_v[k];
+      if (lane == 0) {
+        uint64_t nw[W], vis[W];
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+          nw[i] = s_acc[k][i] & s_need[k][i];
+          any |= nw[i] != 0;
+        }
+        if (any) {
+          load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
+          uint64_t nv2[W];
+#pragma unroll
+          for (int i = 0; i < W; ++i) {
+            nv2[i] = vis[i] | nw[i];
+            uni[i] |= nw[i];
+            pairs += __popcll(nw[i]);
+          }
+          store_mask<W>(g.visited + static_cast<size_t>(v) * W, nv2);
+          store_mask<W>(lv.fnext + static_cast<size_t>(v) * W, nw);
+          record_depth<W, DEPTH>(g, G.V, v, nw, lv.level + 1, true);
+          app = g.stamp[v] < lv.level + 1;
+          g.stamp[v] = lv.level + 1;
+        }
+      }
+      ap.add<OT>(app, v, G, lv, lane);
+    }
+    __syncthreads();
+  }
+  ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
   warp_add(pairs, &g.ctl->lc.new_pairs, lane);
   warp_add(pverts, &g.ctl->lc.pull_vertices, lane);
@@ -1044,6 +1223,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
   const LevelView lv = level_view(g);
   WarpAppender ap;
   const unsigned long long n = ctl->count[lv.par];
+  const int64_t light = push_light_limit(g, G, n);
   uint64_t sel[W];
 #pragma unroll
   for (int i = 0; i < W; ++i) sel[i] = ctl->ssel[i];
@@ -1081,7 +1261,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
       }
     }
     const int64_t deg = end - beg;
-    const bool work = valid && k > 0 && deg > 0 && deg <= G.heavy_degree;
+    const bool work = valid && k > 0 && deg > 0 && deg <= light;
     spairs += work ? static_cast<unsigned long long>(k) * static_cast<unsigned long long>(deg) : 0ULL;
     sactive += static_cast<unsigned long long>(k);
     // vertices with many active queries go to the dense kernel
@@ -1622,25 +1802,6 @@ __device__ __forceinline__ void gather_vec_words(uint32_t bits, int lane,
   }
 }
 
-// Whether the gather screens in-edges by their source's frontier mask: -1
-// when the frontier's out-edges are less than half of all edges, or when its
-// (vertex, slot) entries are sparse (the previous level improved fewer than
-// 1/32 of the frontier's vertices x SSSP slots); screened gathers skip sources
-// with no frontier bit and, within a source row, the 32-slot chunks with none.
-// Otherwise the number of SSSP slots: every source row is read whole, which
-// skips a dependent mask load per 32 in-edges and costs little when almost
-// every (source, slot) is live.
-template <int W>
-__device__ __forceinline__ int gather_screen_qs(const LevelCtl* ctl, const LevelView& lv,
-                                                int64_t E) {
-  int qs = 0;
-#pragma unroll
-  for (int i = 0; i < W; ++i) qs += __popcll(ctl->gsel[i]);
-  if (2 * ctl->edges[lv.par] < static_cast<unsigned long long>(E)) return -1;
-  if (32 * ctl->prev_improved < ctl->count[lv.par] * static_cast<unsigned long long>(qs)) return -1;
-  return qs;
-}
-
 // 32-slot chunks that hold a gathering SSSP slot at this level.
 template <int W>
 __device__ __forceinline__ uint32_t gather_chunks(const LevelCtl* ctl) {
@@ -1650,26 +1811,62 @@ __device__ __forceinline__ uint32_t gather_chunks(const LevelCtl* ctl) {
   return chunk_bits<W>(gs);
 }
 
-// Writes the frontier summary of the current frontier's vertices on levels
-// that screen sources by it (screened SSSP gathers, sparse BFS pulls); other
-// levels return at once.  Words of vertices outside the frontier keep an older
-// level's stamp and read as empty.
+// Whether the gather screens in-edges by their source's frontier chunks (-1)
+// or reads every in-edge's source row whole (the number of gathering slots).
+// With the frontier summary: a whole-row gather reads E x (gathering chunks)
+// row chunks, a screened one only the live ones, which the summary kernel
+// counted (live_chunks); screening pays when fewer than 4/5 of them are live,
+// and costs an 8-byte L2 word per in-edge.  Without it (no summary buffer):
+// screen when the frontier's out-edges are less than half of all edges or its
+// entries are sparse (the previous level improved fewer than 1/32 of the
+// frontier's vertices x SSSP slots), reading the sources' W-word masks.
 template <int W>
+__device__ __forceinline__ int gather_screen_qs(const GroupDev& g, const LevelCtl* ctl,
+                                                const LevelView& lv, int64_t E) {
+  int qs = 0;
+#pragma unroll
+  for (int i = 0; i < W; ++i) qs += __popcll(ctl->gsel[i]);
+  if (g.fsum != nullptr) {
+    const unsigned long long whole =
+        static_cast<unsigned long long>(E) * static_cast<unsigned long long>(__popc(gather_chunks<W>(ctl)));
+    return 5 * ctl->lc.live_chunks < 4 * whole ? -1 : qs;
+  }
+  if (2 * ctl->edges[lv.par] < static_cast<unsigned long long>(E)) return -1;
+  if (32 * ctl->prev_improved < ctl->count[lv.par] * static_cast<unsigned long long>(qs)) return -1;
+  return qs;
+}
+
+// Writes the frontier summary of the current frontier's vertices on SSSP
+// gather levels and sparse BFS pull levels (other levels return at once), and
+// on gather levels counts the live row chunks a screened gather would read
+// (out-degree x gathering chunks with a frontier bit).  Words of vertices
+// outside the frontier keep an older level's stamp and read as empty.
+template <int W, typename OT>
 __global__ void __launch_bounds__(kBlock) k_frontier_summary(GroupDev g, DevGraph G) {
-  const LevelCtl* ctl = g.ctl;
+  LevelCtl* ctl = g.ctl;
   if (ctl->done) return;
   const LevelView lv = level_view(g);
-  const bool sssp = ctl->sdir == kDirPull && gather_screen_qs<W>(ctl, lv, G.E) < 0;
+  const bool sssp = ctl->sdir == kDirPull;
   if (!sssp && !bfs_pull_uses_summary(g, ctl, lv, G.V)) return;
   const unsigned long long n = ctl->count[lv.par];
   const uint64_t stamp = static_cast<uint64_t>(lv.level + 1) << 32;
-  for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-       i < n; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
-    const int32_t v = lv.list[i];
-    uint64_t m[W];
-    load_mask<W>(lv.fcur + static_cast<size_t>(v) * W, m);
-    g.fsum[v] = stamp | chunk_bits<W>(m);
+  const uint32_t gch = gather_chunks<W>(ctl);
+  const int lane = threadIdx.x & 31;
+  unsigned long long live = 0;
+  const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
+  for (unsigned long long i0 = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
+       i0 < n; i0 += stride) {
+    const unsigned long long i = i0 + lane;
+    if (i < n) {
+      const int32_t v = lv.list[i];
+      uint64_t m[W];
+      load_mask<W>(lv.fcur + static_cast<size_t>(v) * W, m);
+      const uint32_t cm = chunk_bits<W>(m);
+      g.fsum[v] = stamp | cm;
+      if (sssp) live += __popc(cm & gch) * degree_of<OT>(G.row, v);
+    }
   }
+  if (sssp) warp_add(live, &ctl->lc.live_chunks, lane);
 }
 
 // Whether the lane reads part r of a source row whose 32-slot chunk bits are
@@ -1809,7 +2006,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   unsigned scanned = 0, verts = 0;
   int32_t pend_v = 0;  // lane i: i-th vertex waiting to be appended
   int pend_n = 0;      // uniform
-  const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const int screen_qs = gather_screen_qs<W>(g, ctl, lv, G.E);
   const uint32_t gch = gather_chunks<W>(ctl);
   const unsigned long long V = static_cast<unsigned long long>(G.V);
   // the next vertex's offsets are loaded while the current one is gathered
@@ -1929,7 +2126,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
   const uint64_t* sb = ctl->gsel;
   uint32_t pmask, smask;
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
-  const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const int screen_qs = gather_screen_qs<W>(g, ctl, lv, G.E);
   const uint32_t gch = gather_chunks<W>(ctl);
   const size_t Qg = static_cast<size_t>(g.Qg);
   const uint32_t* lanebase = g.values + lane * E;
@@ -2151,7 +2348,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   uint32_t pmask, smask;
   gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
-  const int screen_qs = gather_screen_qs<W>(ctl, lv, G.E);
+  const int screen_qs = gather_screen_qs<W>(g, ctl, lv, G.E);
   const uint32_t gch = gather_chunks<W>(ctl);
   if ((kMode == 1 && screen_qs < 0) || (kMode == 2 && screen_qs >= 0)) return;
   const size_t Qg = static_cast<size_t>(g.Qg);
@@ -2281,6 +2478,10 @@ __device__ __forceinline__ void split_sssp_slots(LevelCtl* ctl, int32_t group_di
     ctl->ssel[i] = ctl->sssp_bits[i] & ~gm;
     g_any |= ctl->gsel[i] != 0;
     s_any |= ctl->ssel[i] != 0;
+    for (int h = 0; h < 2; ++h) {
+      ctl->sssp_chunk_levels += static_cast<uint32_t>(ctl->sssp_bits[i] >> (32 * h)) != 0u;
+      ctl->gather_chunk_levels += static_cast<uint32_t>(ctl->gsel[i] >> (32 * h)) != 0u;
+    }
   }
   for (int c = 0; c < 2 * kMaxW; ++c) ctl->cedges[c] = 0;
   ctl->sdir = g_any ? kDirPull : kDirPush;
@@ -2333,6 +2534,8 @@ __device__ void level_end(GroupDev& g) {
   ctl->total.sssp_active += ctl->lc.sssp_active;
   ctl->total.improved += ctl->lc.improved;
   ctl->prev_improved = ctl->lc.improved;
+  ctl->prev_pull_edges = ctl->lc.pull_edges;
+  ctl->prev_dir = ctl->dir;
   ctl->total.spull_vertices += ctl->lc.spull_vertices;
   ctl->total.spull_edges += ctl->lc.spull_edges;
   ctl->lc = LevelCounters{};

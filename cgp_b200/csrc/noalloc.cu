@@ -86,7 +86,7 @@ void run_levels(const GroupDev& g, const DevGraph& G, bool pull, int64_t V, int 
   // the flag is read back every 4 levels.
   for (int chunk = 0;; ++chunk) {
     for (int i = 0; i < 4; ++i) {
-      k_clear_next<W><<<blocks, kBlock, 0, s>>>(g);
+      k_clear_next<W><<<blocks, kBlock, 0, s>>>(g, G.E);
       k_bfs_push<W, OT, kDepthDirect><<<blocks, kBlock, 0, s>>>(g, G);
       if (pull) k_bfs_pull<W, OT, kDepthDirect><<<blocks, kBlock, 0, s>>>(g, G);
       k_level_end<W><<<1, 32, 0, s>>>(g);
@@ -154,7 +154,7 @@ extern "C" cgp_status cgp_bfs_batch_noalloc(const void* row_offsets, int32_t off
     const int64_t V = num_vertices;
     // carve the scratch array
     char* p = static_cast<char*>(base);
-    GroupDev g;
+    GroupDev g{};
     g.ctl = reinterpret_cast<LevelCtl*>(p);
     p += align256(sizeof(LevelCtl));
     g.slots = reinterpret_cast<const SlotDev*>(p);

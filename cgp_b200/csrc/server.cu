@@ -234,6 +234,8 @@ struct cgp_server {
   double admit_ms = 0;
   double retire_ms = 0;
   int64_t retire_passes = 0;
+  int64_t sssp_chunk_levels = 0;
+  int64_t gather_chunk_levels = 0;
   int64_t state_bytes = 0;
   bool wcc_ready = false;
   std::string fatal;
@@ -248,7 +250,7 @@ struct cgp_server {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   void loop();
-  int pick_slot();
+  int pick_slot(int kind);
   void finish_wcc(std::vector<uint64_t>& tickets);
   void retire(std::vector<int>& slots_to_retire, bool forced);
 };
@@ -285,7 +287,7 @@ RetireFn pick_retire(int W) {
 }
 
 GroupDev server_dev(cgp_server* sv) {
-  GroupDev g;
+  GroupDev g{};
   Workspace* ws = sv->ws.get();
   g.visited = ws->visited.as<uint64_t>();
   g.fbuf0 = ws->fbuf0.as<uint64_t>();
@@ -340,30 +342,39 @@ void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
   done_cv.notify_all();
 }
 
-// A free slot for the next admission (mu held), or -1.  Slots are taken in
-// 32-slot cohorts, so that requests that arrive together share a chunk and
-// pass through their sparse and dense phases together (what the per-chunk
-// SSSP direction needs): first a chunk already taken by this admission pass,
-// then an empty chunk, then the chunk whose occupants were admitted last.
-int cgp_server::pick_slot() {
+// A free slot for the next admission of a request of `kind` (mu held), or -1.
+// Slots are taken in 32-slot cohorts of one class (SSSP, or BFS-like: BFS and
+// k-hop), so that requests that arrive together share a chunk with requests
+// of their own class and pass through their sparse and dense phases together:
+// an SSSP chunk then gathers only at its own dense levels (the SSSP direction
+// is decided per chunk) and its row chunks hold SSSP slots only.  Preference:
+// a chunk of the class already taken in this admission pass, an empty chunk,
+// the chunk of the class whose occupants were admitted last, any free slot.
+int cgp_server::pick_slot(int kind) {
+  const bool sssp = kind == CGP_KIND_SSSP;
   int best = -1;
   long long best_key = -1;
   for (int c0 = 0; c0 < S; c0 += 32) {
     const int c1 = std::min(S, c0 + 32);
     int free_slot = -1, occupied = 0, newest = -1;
-    bool this_pass = false;
+    bool this_pass = false, same = true;
     for (int i = c0; i < c1; ++i) {
       if (slot_ticket[i] < 0) {
         if (free_slot < 0) free_slot = i;
         continue;
       }
       ++occupied;
-      const int al = reqs[static_cast<uint64_t>(slot_ticket[i])].admit_level;
-      if (al < 0) this_pass = true;  // level set once the admission kernel ran
-      newest = std::max(newest, al);
+      const Request& r = reqs[static_cast<uint64_t>(slot_ticket[i])];
+      same &= (r.q.kind == CGP_KIND_SSSP) == sssp;
+      if (r.admit_level < 0) this_pass = true;  // level set once the admission kernel ran
+      newest = std::max(newest, r.admit_level);
     }
     if (free_slot < 0) continue;
-    const long long key = this_pass ? (3LL << 40) : occupied == 0 ? (2LL << 40) : newest;
+    long long key;
+    if (occupied == 0) key = 3LL << 40;
+    else if (same && this_pass) key = 4LL << 40;
+    else if (same) key = (2LL << 40) + newest;
+    else key = newest;
     if (key > best_key) {
       best_key = key;
       best = free_slot;
@@ -461,7 +472,7 @@ void cgp_server::loop() {
             wcc_tickets.push_back(tk);
             continue;
           }
-          const int s = pick_slot();
+          const int s = pick_slot(r.q.kind);
           if (s < 0) break;
           pending.pop_front();
           slot_ticket[s] = static_cast<int64_t>(tk);
@@ -506,6 +517,8 @@ void cgp_server::loop() {
       ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
       busy_ms += now_ms() - tb;
       levels = c.level;
+      sssp_chunk_levels = static_cast<int64_t>(c.sssp_chunk_levels);
+      gather_chunk_levels = static_cast<int64_t>(c.gather_chunk_levels);
       // converged: occupied, admitted before the current level, no frontier bit
       std::vector<int> conv, forced;
       {
@@ -735,6 +748,8 @@ cgp_status cgp_server_get_stats(cgp_server* sv, cgp_server_stats* st) {
   st->admit_ms = sv->admit_ms;
   st->retire_ms = sv->retire_ms;
   st->retire_passes = sv->retire_passes;
+  st->sssp_chunk_levels = sv->sssp_chunk_levels;
+  st->gather_chunk_levels = sv->gather_chunk_levels;
   for (int c = 0; c < 12; ++c) st->kernel_ms[c] = sv->kt && c < kNumClasses ? sv->kt->ms[c] : 0.0;
   return CGP_OK;
 }

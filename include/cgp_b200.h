@@ -115,7 +115,9 @@ typedef struct {
                                    chunk's own frontier (1), or for the whole group (-1);
                                    0 = auto: per chunk in the serving loop, whole group in
                                    batch runs                                              */
-  int32_t reserved;
+  int32_t bfs_pull_form;      /* light-vertex BFS pull: 0 = CTA chunks on pull levels that read
+                                 most in-edges, a lane per vertex elsewhere; -1 = a lane per
+                                 vertex on every pull level                                  */
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 
@@ -373,6 +375,8 @@ typedef struct {
   double retire_ms;          /* host time spent retiring slots and copying results   */
   int64_t retire_passes;     /* snapshot-and-reset passes over the vertices          */
   double kernel_ms[12];      /* per kernel class when created with profile_kernels   */
+  int64_t sssp_chunk_levels;   /* sum over levels of 32-slot chunks holding SSSP slots */
+  int64_t gather_chunk_levels; /* ... of those chunks, the ones whose SSSP slots gathered */
 } cgp_server_stats;
 cgp_status cgp_server_get_stats(cgp_server* s, cgp_server_stats* st);
 
