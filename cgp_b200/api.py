@@ -298,7 +298,7 @@ class RunOptions:
     light_chunks: bool = True
     level_loop: str = "auto"    # "auto", "chunks" (host-checked graph chunks), "device"
     sssp_chunk_direction: int = 0  # 1 per 32-slot chunk, -1 whole group, 0 auto (serving: chunk)
-    bfs_pull_chunks: bool = True   # CTA-chunked light-vertex BFS pull on levels that read most edges
+    bfs_pull_chunks: bool = False  # CTA-chunked light-vertex BFS pull on levels that read most edges
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -327,7 +327,7 @@ class RunOptions:
         o.level_loop = {"auto": N.LOOP_AUTO, "chunks": N.LOOP_CHUNKS,
                         "device": N.LOOP_DEVICE}[self.level_loop]
         o.sssp_chunk_direction = int(self.sssp_chunk_direction)
-        o.bfs_pull_form = 0 if self.bfs_pull_chunks else -1
+        o.bfs_pull_form = 1 if self.bfs_pull_chunks else 0
         o.stream = self.stream or None
         return o
 

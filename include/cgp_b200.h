@@ -115,9 +115,9 @@ typedef struct {
                                    chunk's own frontier (1), or for the whole group (-1);
                                    0 = auto: per chunk in the serving loop, whole group in
                                    batch runs                                              */
-  int32_t bfs_pull_form;      /* light-vertex BFS pull: 0 = CTA chunks on pull levels that read
-                                 most in-edges, a lane per vertex elsewhere; -1 = a lane per
-                                 vertex on every pull level                                  */
+  int32_t bfs_pull_form;      /* light-vertex BFS pull: 0 = a lane per vertex on every pull
+                                 level; 1 = CTA chunks on pull levels that read most in-edges
+                                 (measured slower on R-MAT: kept as an option)               */
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 

@@ -658,3 +658,16 @@ def test_sssp_direction_per_chunk_f32_grid(grid_paths):
                                                        level_loop=loop), layout="query")
         ref, _ = oracle.batch("sssp", g, src)
         np.testing.assert_array_equal(r.values.view(np.float32), ref)
+
+
+@pytest.mark.parametrize("nq", [1, 64, 200, 256])
+@pytest.mark.parametrize("depth", ["planes", "direct"])
+def test_bfs_chunked_pull_option(rmat_u32, nq, depth):
+    """The CTA-chunked light-vertex pull (opt-in) gives the oracle's depths."""
+    g, graph = rmat_u32
+    src = g.pick_sources(nq, seed=90 + nq)
+    ref, _ = oracle.batch("bfs", g, src)
+    for ratio in (0.01, 0.2):
+        r = _bfs(src, graph, cgp.RunOptions(bfs_pull_chunks=True, pull_edge_ratio=ratio,
+                                            depth_mode=depth, heavy_degree=64))
+        np.testing.assert_array_equal(r.values, ref)
