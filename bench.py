@@ -116,6 +116,8 @@ def parse_args():
     p.add_argument("--serve-slots", type=int, default=256)
     p.add_argument("--sssp-chunk-direction", type=int, default=0,
                    help="SSSP gather/scatter per 32-slot chunk (1), per group (-1), auto (0)")
+    p.add_argument("--serve-cohorts", action="store_true",
+                   help="serving: admit only into wholly free 32-slot chunks")
     p.add_argument("--serve-profile", action="store_true",
                    help="time the serving loop's kernel classes (slower: no CUDA graphs)")
     a = p.parse_args()
@@ -577,6 +579,7 @@ def run_serve(args):
                                            heavy_degree=args.heavy_degree,
                                            sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
                                            sssp_chunk_direction=args.sssp_chunk_direction,
+                                           serve_cohorts=args.serve_cohorts,
                                            profile_kernels=args.serve_profile)) as srv:
         poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
@@ -602,6 +605,7 @@ def run_serve(args):
             "sssp_direction": {1: "per 32-slot chunk", -1: "per group"}.get(
                 args.sssp_chunk_direction, "auto (per 32-slot chunk)"),
             "sssp_pull_edge_ratio": args.sssp_pull_edge_ratio,
+            "admission": "whole 32-slot cohorts" if args.serve_cohorts else "any free slot",
             "seconds_per_rate": args.serve_seconds, "rates": rows, "graph_gen_s": gen_s}
     print(json.dumps(line), flush=True)
     if args.json_out:

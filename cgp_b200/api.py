@@ -299,6 +299,7 @@ class RunOptions:
     level_loop: str = "auto"    # "auto", "chunks" (host-checked graph chunks), "device"
     sssp_chunk_direction: int = 0  # 1 per 32-slot chunk, -1 whole group, 0 auto (serving: chunk)
     bfs_pull_chunks: bool = False  # CTA-chunked light-vertex BFS pull on levels that read most edges
+    serve_cohorts: bool = False    # serving: admit only into wholly free 32-slot chunks
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -328,6 +329,7 @@ class RunOptions:
                         "device": N.LOOP_DEVICE}[self.level_loop]
         o.sssp_chunk_direction = int(self.sssp_chunk_direction)
         o.bfs_pull_form = 1 if self.bfs_pull_chunks else 0
+        o.serve_admission = 1 if self.serve_cohorts else 0
         o.stream = self.stream or None
         return o
 

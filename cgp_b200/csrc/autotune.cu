@@ -94,7 +94,7 @@ extern "C" cgp_status cgp_autotune(cgp_graph* graph, const cgp_query* sample, in
     }
   }
   if (st == CGP_OK) {
-    for (int h : {512, 1024, 4096, 16384}) {
+    for (int h : {128, 256, 512, 1024, 4096, 16384}) {
       cgp_options c = best;
       c.heavy_degree = h;
       time_run(graph, sample, n, c, out, 1, &st);  // builds the heavy table once

@@ -369,6 +369,8 @@ int cgp_server::pick_slot() {
       newest = std::max(newest, al);
     }
     if (free_slot < 0) continue;
+    // whole cohorts: a chunk with occupants from earlier passes takes no one
+    if (o.serve_admission == 1 && occupied > 0 && !this_pass) continue;
     const long long key = this_pass ? (3LL << 40) : occupied == 0 ? (2LL << 40) : newest;
     if (key > best_key) {
       best_key = key;

@@ -118,6 +118,10 @@ typedef struct {
   int32_t bfs_pull_form;      /* light-vertex BFS pull: 0 = a lane per vertex on every pull
                                  level; 1 = CTA chunks on pull levels that read most in-edges
                                  (measured slower on R-MAT: kept as an option)               */
+  int32_t serve_admission;    /* serving loop: 0 = any free slot, preferring the chunk of the
+                                 latest admissions; 1 = whole 32-slot cohorts: requests enter
+                                 only chunks whose slots are all free                        */
+  int32_t reserved;
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 
