@@ -26,6 +26,7 @@ enum : int32_t { kWeightNone = 0, kWeightU32 = 1, kWeightF32 = 2 };
 enum : uint32_t {
   kStatusPlanesExhausted = 1u,  // depth planes too few for the level reached
   kStatusLevelCap = 2u,         // a device-looped traversal reached its level cap
+  kStatusQueueOverflow = 4u,    // the heavy frontier queue was full (entry dropped)
 };
 
 struct LevelProfile {
@@ -155,6 +156,7 @@ struct GroupDev {
   int32_t* dense_list; // [V] SSSP frontier vertices with many active bits
   int32_t* hq_vertex;  // [n_heavy] heavy vertices of the current frontier
   int64_t* hq_start;   // [n_heavy] their first chunk in the level's chunk space
+  int64_t hq_cap;      // entries of hq_vertex / hq_start
   LevelCtl* ctl;
   LevelProfile* prof;
   const SlotDev* slots;

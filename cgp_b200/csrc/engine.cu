@@ -564,6 +564,7 @@ GroupDev group_dev(Workspace* ws, const GroupSpec& spec, bool profiles) {
   g.dense_list = ws->dense.as<int32_t>();
   g.hq_vertex = ws->hq_vertex.as<int32_t>();
   g.hq_start = ws->hq_start.as<int64_t>();
+  g.hq_cap = static_cast<int64_t>(ws->hq_start.bytes / sizeof(int64_t));
   g.ctl = ws->ctl.as<LevelCtl>();
   g.prof = profiles ? ws->prof.as<LevelProfile>() : nullptr;
   g.slots = ws->slots.as<SlotDev>();
@@ -606,8 +607,9 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
     moved |= ws->stamp.ensure(static_cast<size_t>(V) * 4);
     moved |= ws->hacc.ensure(static_cast<size_t>(std::max(1, hp.pheavy.n)) * W * 8);
     moved |= ws->fsum.ensure(static_cast<size_t>(V) * 8);
-    // heavy-queue capacity: every heavy vertex, or a whole small frontier
-    const size_t hq_cap = std::max<size_t>(std::max(1, hp.heavy.n), kSmallFrontier);
+    // heavy-queue capacity: every heavy vertex, and every vertex of out-degree
+    // > 32 (small or skewed frontiers queue those)
+    const size_t hq_cap = std::max<size_t>(std::max<int64_t>(1, hp.heavy.n), g->n_deg32);
     moved |= ws->hq_vertex.ensure(hq_cap * 4);
     moved |= ws->hq_start.ensure(hq_cap * 8);
     if (spec.has_sssp) moved |= ws->dense.ensure(static_cast<size_t>(V) * 4);
@@ -979,6 +981,7 @@ cgp_status cgp_graph_create(const void* row_offsets, int32_t offset_bytes,
     for (int64_t v = 0; v < num_vertices; ++v) {
       if (hrow[v + 1] < hrow[v]) throw ApiError{CGP_ERR_INVALID_ARG, "row_offsets not monotone"};
       G.max_degree = std::max(G.max_degree, hrow[v + 1] - hrow[v]);
+      G.n_deg32 += hrow[v + 1] - hrow[v] > 32 ? 1 : 0;
     }
     std::vector<int32_t> hcol(num_edges);
     if (num_edges > 0)

@@ -138,6 +138,7 @@ struct GraphImpl {
   int num_sms = 148;
   int64_t V = 0, E = 0;
   int64_t max_degree = 0;  // largest out-degree of the traversal CSR
+  int64_t n_deg32 = 0;     // vertices of out-degree > 32 (heavy-queue capacity)
   int offset_bytes = 4;
   int weight_kind = CGP_WEIGHT_NONE;
   bool symmetric = false;

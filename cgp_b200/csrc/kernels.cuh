@@ -205,16 +205,19 @@ __device__ __forceinline__ LevelView level_view(const GroupDev& g) {
 
 // Frontier vertices that a push level's tile kernels expand themselves: out-
 // degree at most the returned limit.  Larger lists go to the heavy queue as
-// kHeavyChunk-edge CTA work items: lists above heavy_degree always, and on a
-// small frontier (<= kSmallFrontier vertices, e.g. the sources' level) every
-// list above 32 edges, so that a few long lists are not each walked by a
-// single warp while most warps of the grid have nothing to do.
+// kHeavyChunk-edge CTA work items: lists above heavy_degree always, and every
+// list above 32 edges when the frontier is small (<= kSmallFrontier vertices,
+// e.g. the sources' level) or skewed (more than 64 out-edges per vertex on
+// average, e.g. the hubs reached by the sources): there a tile of 32 such
+// vertices would be one warp's serial work while most warps of the grid have
+// nothing to do.  (The heavy queue holds every vertex of out-degree > 32.)
 constexpr unsigned long long kSmallFrontier = 4096;
 
 __device__ __forceinline__ int64_t push_light_limit(const GroupDev& g, const DevGraph& G,
-                                                    unsigned long long count) {
-  return (g.hq_vertex != nullptr && count <= kSmallFrontier && G.heavy_degree > 32)
-             ? 32 : G.heavy_degree;
+                                                    unsigned long long count,
+                                                    unsigned long long edges) {
+  const bool spread = count <= kSmallFrontier || edges > 64ULL * count;
+  return (g.hq_vertex != nullptr && spread && G.heavy_degree > 32) ? 32 : G.heavy_degree;
 }
 
 // ------------------------------------------------------- depth recording
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push(GroupDev g, DevGraph G) {
   const LevelView lv = level_view(g);
   WarpAppender ap;
   const unsigned long long n = ctl->count[lv.par];
-  const int64_t light = push_light_limit(g, G, n);
+  const int64_t light = push_light_limit(g, G, n, ctl->edges[lv.par]);
   uint64_t sel[W];
 #pragma unroll
   for (int i = 0; i < W; ++i) sel[i] = ctl->bfs_bits[i] & ctl->expand[i];
@@ -473,7 +476,7 @@ __global__ void __launch_bounds__(kBlock) k_heavy_queue(GroupDev g, DevGraph G) 
   if (ctl->done || (ctl->dir != kDirPush && !ctl->sscatter)) return;
   const LevelView lv = level_view(g);
   const unsigned long long n = ctl->count[lv.par];
-  const int64_t light = push_light_limit(g, G, n);
+  const int64_t light = push_light_limit(g, G, n, ctl->edges[lv.par]);
   for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
        i < n; i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
     const int32_t u = lv.list[i];
@@ -482,6 +485,10 @@ __global__ void __launch_bounds__(kBlock) k_heavy_queue(GroupDev g, DevGraph G) 
     const unsigned long long chunks = static_cast<unsigned long long>((deg + kHeavyChunk - 1) / kHeavyChunk);
     const unsigned long long old = atomicAdd(&ctl->hq_packed, (1ULL << kQueueShift) | chunks);
     const unsigned long long slot = old >> kQueueShift;
+    if (slot >= static_cast<unsigned long long>(g.hq_cap)) {  // cannot happen with unique lists
+      atomicOr(&ctl->status, kStatusQueueOverflow);
+      continue;
+    }
     g.hq_vertex[slot] = u;
     g.hq_start[slot] = static_cast<int64_t>(old & ((1ULL << kQueueShift) - 1));
   }
@@ -505,7 +512,8 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push_heavy(GroupDev g, DevGraph 
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->dir != kDirPush) return;
   const unsigned long long hq = ctl->hq_packed;
-  const int nq = static_cast<int>(hq >> kQueueShift);
+  const int nq = static_cast<int>(min(static_cast<long long>(hq >> kQueueShift),
+                                      static_cast<long long>(g.hq_cap)));
   const int64_t nchunks = static_cast<int64_t>(hq & ((1ULL << kQueueShift) - 1));
   if (nq == 0) return;
   const LevelView lv = level_view(g);
@@ -1223,7 +1231,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push(GroupDev g, DevGraph G) {
   const LevelView lv = level_view(g);
   WarpAppender ap;
   const unsigned long long n = ctl->count[lv.par];
-  const int64_t light = push_light_limit(g, G, n);
+  const int64_t light = push_light_limit(g, G, n, ctl->edges[lv.par]);
   uint64_t sel[W];
 #pragma unroll
   for (int i = 0; i < W; ++i) sel[i] = ctl->ssel[i];
@@ -1347,7 +1355,8 @@ __global__ void __launch_bounds__(kBlock) k_sssp_push_heavy(GroupDev g, DevGraph
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || !ctl->sscatter) return;
   const unsigned long long hq = ctl->hq_packed;
-  const int nq = static_cast<int>(hq >> kQueueShift);
+  const int nq = static_cast<int>(min(static_cast<long long>(hq >> kQueueShift),
+                                      static_cast<long long>(g.hq_cap)));
   const int64_t nchunks = static_cast<int64_t>(hq & ((1ULL << kQueueShift) - 1));
   if (nq == 0) return;
   const LevelView lv = level_view(g);

@@ -139,3 +139,20 @@ def test_server_slots_bounded_by_memory(rmat):
         assert 1 <= st["slots"] < 512 and st["state_bytes"] <= budget
         t = s.submit(cgp.QueryDescriptor(int(g.pick_sources(1, seed=3)[0]), "bfs"))
         assert s.wait(t, 60000).state == "done"
+
+
+def test_whole_cohort_admission_matches_oracle(rmat):
+    """Admission in whole 32-slot cohorts (requests enter only wholly free
+    chunks) gives every request its exact result."""
+    g, graph = rmat
+    src = g.pick_sources(80, seed=61)
+    kinds = ["bfs", "sssp", "khop"]
+    descs = [cgp.QueryDescriptor(int(s), kinds[i % 3], 2 + i % 4 if i % 3 == 2 else 0)
+             for i, s in enumerate(src)]
+    outs = [np.zeros(g.num_vertices, np.uint32) for _ in descs]
+    with cgp.Server(graph, slots=64, options=cgp.RunOptions(serve_cohorts=True)) as s:
+        tickets = [s.submit(d, o) for d, o in zip(descs, outs)]
+        s.drain(timeout_ms=120000)
+        assert all(s.poll(t).state == "done" for t in tickets)
+    for d, o in zip(descs, outs):
+        np.testing.assert_array_equal(o, _expected(g, d))
