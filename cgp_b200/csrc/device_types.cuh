@@ -138,6 +138,7 @@ struct DevGraph {
   const int32_t* plight;             // light vertices of the pull CSR (chunked gathers)
   const int32_t* plight_chunk_start; // [n_plight_chunks + 1]
   int32_t n_plight_chunks;
+  int32_t n_pmid;                    // plight[0 .. n_pmid) have in-degree > 32 (BFS pull mid kernel)
 };
 
 struct GroupDev {

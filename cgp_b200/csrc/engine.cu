@@ -153,6 +153,7 @@ DevGraph GraphImpl::dev_graph(int64_t h) {
   d.plight = hp.plight.vertices.as<int32_t>();
   d.plight_chunk_start = hp.plight.chunk_start.as<int32_t>();
   d.n_plight_chunks = hp.plight.chunks;
+  d.n_pmid = hp.plight.n_mid;
   d.heavy_degree = h;
   return d;
 }
@@ -217,6 +218,8 @@ void build_light_chunks(const std::vector<int64_t>& row, int64_t V, int64_t h, L
   if (cur_v > 0) cs.push_back(static_cast<int32_t>(vs.size()));
   t.n = static_cast<int32_t>(vs.size());
   t.chunks = static_cast<int32_t>(cs.size()) - 1;
+  t.n_mid = 0;
+  while (t.n_mid < t.n && row[vs[t.n_mid] + 1] - row[vs[t.n_mid]] > 32) ++t.n_mid;
   t.vertices.ensure(std::max<size_t>(vs.size(), 1) * sizeof(int32_t));
   t.chunk_start.ensure(cs.size() * sizeof(int32_t));
   if (!vs.empty())
@@ -333,6 +336,7 @@ struct Grids {
   int gather_chunked;
   int gather_heavy_vec2;
   int bfs_chunked;
+  int bfs_mid;
 };
 
 struct LevelLaunch {
@@ -394,6 +398,10 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
       if (kt) kt->mark(kClassBfsPull, s);
       k_bfs_pull<W, OT, DEPTH><<<t, kBlock, 0, s>>>(L.g, L.G);
       ++n;
+      if (L.G.n_pmid > 0) {  // in-degree 33 .. heavy_degree: warp per vertex
+        k_bfs_pull_mid<W, OT, DEPTH><<<L.gr.bfs_mid, kBlock, 0, s>>>(L.g, L.G);
+        ++n;
+      }
       if (L.bfs_chunked) {  // each of the two forms returns at once on the other's levels
         k_bfs_pull_chunked<W, OT, DEPTH><<<L.gr.bfs_chunked, kBlock, 0, s>>>(L.g, L.G);
         ++n;
@@ -469,9 +477,10 @@ template <int W, typename OT, int DEPTH, int WK>
 Grids grids_t(int sms) {
   static int tile = 0, heavy = 0, dense = 0, dense2 = 0, gather = 0, gather_heavy = 0;
   static int gather_vec = 0, gather_heavy_vec = 0, gather_chunked = 0, gather_heavy_vec2 = 0;
-  static int bfs_chunked = 0;
+  static int bfs_chunked = 0, bfs_mid = 0;
   if (tile == 0) {
     bfs_chunked = occupancy_grid(k_bfs_pull_chunked<W, OT, DEPTH>, sms);
+    bfs_mid = occupancy_grid(k_bfs_pull_mid<W, OT, DEPTH>, sms);
     if constexpr (W <= 4) gather_chunked = occupancy_grid(k_sssp_pull_chunked<W, OT, WK>, sms);
     gather_vec = occupancy_grid(k_sssp_pull_vec<W, OT, WK>, sms);
     gather_heavy_vec = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK, (W <= 4 ? 1 : 0)>, sms);
@@ -500,6 +509,7 @@ Grids grids_t(int sms) {
   g.gather_chunked = gather_chunked;
   g.gather_heavy_vec2 = gather_heavy_vec2;
   g.bfs_chunked = bfs_chunked;
+  g.bfs_mid = bfs_mid;
   return g;
 }
 

@@ -59,6 +59,7 @@ struct LightChunks {
   DevBuf chunk_start;  // int32 [chunks + 1] positions in `vertices`
   int32_t n = 0;
   int32_t chunks = 0;
+  int32_t n_mid = 0;   // the first n_mid have in-degree > 32
 };
 
 struct HeavyPair {

@@ -666,7 +666,9 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
       for (int i = 0; i < W; ++i) need[i] = ~vis[i] & act[i];
     }
     const int64_t deg = end - beg;
-    const bool heavy = deg > G.heavy_degree;
+    // heavy lists are the heavy kernels'; lists of 33 .. heavy_degree in-edges
+    // are k_bfs_pull_mid's when the light table lists them
+    const bool heavy = deg > G.heavy_degree || (G.n_pmid > 0 && deg > 32);
     const bool work = valid && !heavy && deg > 0 && mask_any<W>(need);
     pverts += work ? 1 : 0;
     if (work && deg <= 32) {
@@ -888,6 +890,94 @@ __global__ void __launch_bounds__(kBlock) k_bfs_pull_chunked(GroupDev g, DevGrap
       ap.add<OT>(app, v, G, lv, lane);
     }
     __syncthreads();
+  }
+  ap.flush<OT>(G, lv, lane);
+  flush_union<W>(uni, lv.nactive, lane);
+  warp_add(pairs, &g.ctl->lc.new_pairs, lane);
+  warp_add(pverts, &g.ctl->lc.pull_vertices, lane);
+  warp_add(pedges, &g.ctl->lc.pull_edges, lane);
+}
+
+// Pull level, vertices with 33 .. heavy_degree in-edges (the first n_pmid
+// entries of the pull CSR's light table, largest first): a warp per vertex,
+// 64 in-edges per step (two column -> mask loads in flight per lane, then a
+// warp OR-reduce and the early-exit test), one commit per vertex.  In the
+// lane-per-vertex tile kernel these lists were a warp's serial work with one
+// 32-edge step in flight; here they have a kernel and a register budget of
+// their own.  Every listed vertex's next mask is written (zero when nothing
+// is new), as the tile kernel does for its vertices.
+template <int W, typename OT, int DEPTH>
+__global__ void __launch_bounds__(kBlock, 3) k_bfs_pull_mid(GroupDev g, DevGraph G) {
+  const LevelCtl* ctl = g.ctl;
+  if (ctl->done || ctl->dir != kDirPull || G.n_pmid == 0) return;
+  if (G.n_plight_chunks > 0 && bfs_pull_chunked_level(ctl, G.E)) return;
+  const LevelView lv = level_view(g);
+  uint64_t act[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i)
+    act[i] = ctl->active[lv.par][i] & ctl->bfs_bits[i] & ctl->expand[i];
+  const bool use_sum = bfs_pull_uses_summary(g, ctl, lv, G.V);
+  const int lane = threadIdx.x & 31;
+  const long long gw = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+  WarpAppender ap;
+  uint64_t uni[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) uni[i] = 0;
+  unsigned long long pairs = 0, pverts = 0, pedges = 0;
+  for (long long i = gw; i < G.n_pmid; i += nwarps) {
+    const int32_t v = G.plight[i];
+    uint64_t vis[W], need[W];
+    load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
+    bool any = false;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      need[k] = ~vis[k] & act[k];
+      any |= need[k] != 0;
+    }
+    uint64_t a[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) a[k] = 0;
+    if (any) {  // uniform
+      if (lane == 0) ++pverts;
+      const int64_t beg = row_at<OT>(G.prow, v);
+      const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+      const uint32_t nch = chunk_bits<W>(need);
+      for (int64_t e0 = beg; e0 < end; e0 += 64) {
+        int32_t u0 = -1, u1 = -1;
+        if (e0 + lane < end) u0 = G.pcol[e0 + lane];
+        if (e0 + 32 + lane < end) u1 = G.pcol[e0 + 32 + lane];
+        pedges += (u0 >= 0 ? 1 : 0) + (u1 >= 0 ? 1 : 0);
+        if (use_sum) {
+          if (u0 >= 0 && !(summary_chunks(g.fsum, lv.level, u0) & nch)) u0 = -1;
+          if (u1 >= 0 && !(summary_chunks(g.fsum, lv.level, u1) & nch)) u1 = -1;
+        }
+        uint64_t f0[W], f1[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          f0[k] = 0;
+          f1[k] = 0;
+        }
+        if (u0 >= 0) load_mask<W>(lv.fcur + static_cast<size_t>(u0) * W, f0);
+        if (u1 >= 0) load_mask<W>(lv.fcur + static_cast<size_t>(u1) * W, f1);
+#pragma unroll
+        for (int k = 0; k < W; ++k) a[k] |= (f0[k] | f1[k]) & need[k];
+        warp_or_reduce<W>(a);
+        bool full = true;
+#pragma unroll
+        for (int k = 0; k < W; ++k) full &= a[k] == need[k];
+        if (full) break;
+      }
+    }
+    bool app = false;
+    if (lane == 0) {
+      uint64_t nw[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) nw[k] = a[k] & need[k];
+      pull_commit<W, DEPTH>(g, G.V, lv, v, vis, nw, uni, pairs);
+      app = mask_any<W>(nw);
+    }
+    ap.add<OT>(app, v, G, lv, lane);
   }
   ap.flush<OT>(G, lv, lane);
   flush_union<W>(uni, lv.nactive, lane);
