@@ -116,8 +116,8 @@ def parse_args():
     p.add_argument("--serve-slots", type=int, default=256)
     p.add_argument("--sssp-chunk-direction", type=int, default=0,
                    help="SSSP gather/scatter per 32-slot chunk (1), per group (-1), auto (0)")
-    p.add_argument("--serve-cohorts", action="store_true",
-                   help="serving: admit only into wholly free 32-slot chunks")
+    p.add_argument("--serve-admission", default="slots", choices=["slots", "chunks", "group"],
+                   help="serving admission: any free slot, whole 32-slot chunks, or whole groups")
     p.add_argument("--serve-profile", action="store_true",
                    help="time the serving loop's kernel classes (slower: no CUDA graphs)")
     a = p.parse_args()
@@ -579,7 +579,7 @@ def run_serve(args):
                                            heavy_degree=args.heavy_degree,
                                            sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
                                            sssp_chunk_direction=args.sssp_chunk_direction,
-                                           serve_cohorts=args.serve_cohorts,
+                                           serve_admission=args.serve_admission,
                                            profile_kernels=args.serve_profile)) as srv:
         poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
@@ -605,7 +605,8 @@ def run_serve(args):
             "sssp_direction": {1: "per 32-slot chunk", -1: "per group"}.get(
                 args.sssp_chunk_direction, "auto (per 32-slot chunk)"),
             "sssp_pull_edge_ratio": args.sssp_pull_edge_ratio,
-            "admission": "whole 32-slot cohorts" if args.serve_cohorts else "any free slot",
+            "admission": {"slots": "any free slot", "chunks": "whole 32-slot cohorts",
+                          "group": "group cohorts"}[args.serve_admission],
             "seconds_per_rate": args.serve_seconds, "rates": rows, "graph_gen_s": gen_s}
     print(json.dumps(line), flush=True)
     if args.json_out:

@@ -299,7 +299,8 @@ class RunOptions:
     level_loop: str = "auto"    # "auto", "chunks" (host-checked graph chunks), "device"
     sssp_chunk_direction: int = 0  # 1 per 32-slot chunk, -1 whole group, 0 auto (serving: chunk)
     bfs_pull_chunks: bool = False  # CTA-chunked light-vertex BFS pull on levels that read most edges
-    serve_cohorts: bool = False    # serving: admit only into wholly free 32-slot chunks
+    serve_admission: str = "slots"  # serving: "slots" (any free slot), "chunks" (whole 32-slot
+                                    # cohorts) or "group" (a new cohort only in an empty group)
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -329,7 +330,9 @@ class RunOptions:
                         "device": N.LOOP_DEVICE}[self.level_loop]
         o.sssp_chunk_direction = int(self.sssp_chunk_direction)
         o.bfs_pull_form = 1 if self.bfs_pull_chunks else 0
-        o.serve_admission = 1 if self.serve_cohorts else 0
+        if self.serve_admission not in ("slots", "chunks", "group"):
+            raise ValueError("serve_admission must be slots, chunks or group")
+        o.serve_admission = {"slots": 0, "chunks": 1, "group": 2}[self.serve_admission]
         o.stream = self.stream or None
         return o
 

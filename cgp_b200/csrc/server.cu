@@ -352,6 +352,14 @@ void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
 // offered, since a saturated server refills single freed slots and an
 // all-SSSP chunk then gathers at most levels.)
 int cgp_server::pick_slot() {
+  // group cohorts: a new cohort starts only in an empty group (the requests
+  // of this admission pass join it); then every gather level of the group is
+  // shared by all its SSSP requests
+  if (o.serve_admission == 2) {
+    for (int i = 0; i < S; ++i)
+      if (slot_ticket[i] >= 0 && reqs[static_cast<uint64_t>(slot_ticket[i])].admit_level >= 0)
+        return -1;
+  }
   int best = -1;
   long long best_key = -1;
   for (int c0 = 0; c0 < S; c0 += 32) {

@@ -120,7 +120,8 @@ typedef struct {
                                  (measured slower on R-MAT: kept as an option)               */
   int32_t serve_admission;    /* serving loop: 0 = any free slot, preferring the chunk of the
                                  latest admissions; 1 = whole 32-slot cohorts: requests enter
-                                 only chunks whose slots are all free                        */
+                                 only chunks whose slots are all free; 2 = group cohorts:
+                                 requests enter only an empty group, all pending at once     */
   int32_t reserved;
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;

@@ -141,16 +141,18 @@ def test_server_slots_bounded_by_memory(rmat):
         assert s.wait(t, 60000).state == "done"
 
 
-def test_whole_cohort_admission_matches_oracle(rmat):
+@pytest.mark.parametrize("policy", ["chunks", "group"])
+def test_cohort_admission_matches_oracle(rmat, policy):
     """Admission in whole 32-slot cohorts (requests enter only wholly free
-    chunks) gives every request its exact result."""
+    chunks) or group cohorts (only an empty group takes requests) gives every
+    request its exact result."""
     g, graph = rmat
     src = g.pick_sources(80, seed=61)
     kinds = ["bfs", "sssp", "khop"]
     descs = [cgp.QueryDescriptor(int(s), kinds[i % 3], 2 + i % 4 if i % 3 == 2 else 0)
              for i, s in enumerate(src)]
     outs = [np.zeros(g.num_vertices, np.uint32) for _ in descs]
-    with cgp.Server(graph, slots=64, options=cgp.RunOptions(serve_cohorts=True)) as s:
+    with cgp.Server(graph, slots=64, options=cgp.RunOptions(serve_admission=policy)) as s:
         tickets = [s.submit(d, o) for d, o in zip(descs, outs)]
         s.drain(timeout_ms=120000)
         assert all(s.poll(t).state == "done" for t in tickets)
