@@ -92,6 +92,7 @@ def parse_args():
     p.add_argument("--impl", default="cgp", choices=["cgp", "reference"])
     p.add_argument("--scale", type=int, default=0, help="override the R-MAT scale")
     p.add_argument("--vertices", type=int, default=0, help="override the Chung-Lu vertex count")
+    p.add_argument("--grid-side", type=int, default=0, help="override the grid's rows and columns")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-one-query", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=2)
@@ -112,11 +113,16 @@ def parse_args():
     p.add_argument("--serve", action="store_true",
                    help="serving workload: R-MAT 24, Poisson arrivals, p50/p99 latency")
     p.add_argument("--serve-rates", default="500,2000,8000")
-    p.add_argument("--serve-seconds", type=float, default=3.0)
+    p.add_argument("--serve-seconds", type=float, default=10.0)
     p.add_argument("--serve-slots", type=int, default=256)
+    p.add_argument("--serve-out", default="device", choices=["device", "none"],
+                   help="serving: write each result to a device buffer (a ring) or discard it")
+    p.add_argument("--serve-out-ring", type=int, default=512)
+    p.add_argument("--serve-groups", type=int, default=0,
+                   help="traversal groups of the serving loop (0 = 1)")
     p.add_argument("--sssp-chunk-direction", type=int, default=0,
                    help="SSSP gather/scatter per 32-slot chunk (1), per group (-1), auto (0)")
-    p.add_argument("--serve-admission", default="slots", choices=["slots", "chunks", "group"],
+    p.add_argument("--serve-admission", default="group", choices=["slots", "chunks", "group"],
                    help="serving admission: any free slot, whole 32-slot chunks, or whole groups")
     p.add_argument("--serve-profile", action="store_true",
                    help="time the serving loop's kernel classes (slower: no CUDA graphs)")
@@ -137,6 +143,8 @@ def workload_spec(args):
         wl["scale"] = args.scale
     if args.vertices and wl["graph"] == "chung_lu":
         wl["vertices"] = args.vertices
+    if args.grid_side and wl["graph"] == "grid":
+        wl["rows"] = wl["cols"] = args.grid_side
     return wl
 
 
@@ -528,13 +536,15 @@ def serve_mix(g, n, seed, allowed=None):
     return out
 
 
-def poisson_run(server, descs, rate, seconds, seed):
+def poisson_run(server, descs, rate, seconds, seed, outs=None):
     """Submits requests at Poisson arrival times for `seconds`, waits for all,
     returns latency percentiles and throughput.  Throughput is the completion
     rate between the first and the last completion: it equals the offered rate
     while latency stays stationary and falls to the service capacity when the
     queue grows (the first request's latency, the pipeline fill, is not
-    charged to the window)."""
+    charged to the window).  The p50 latencies of the first and the last third
+    of the arrivals show whether the queue grows.  With `outs`, request i's
+    result is written to device buffer outs[i % len(outs)] (a ring)."""
     rng = np.random.default_rng(seed)
     n = max(1, int(rate * seconds))
     gaps = rng.exponential(1.0 / rate, n)
@@ -549,10 +559,12 @@ def poisson_run(server, descs, rate, seconds, seed):
                 break
             if target - now > 0.002:
                 time.sleep(target - now - 0.001)
-        tickets.append(server.submit(descs[i % len(descs)]))
+        tickets.append(server.submit(descs[i % len(descs)],
+                                     outs[i % len(outs)] if outs else None))
     server.drain()
     infos = [server.wait(t) for t in tickets]
     lat = np.array([i.latency_ms for i in infos])
+    third = max(1, n // 3)
     done = [i for i in infos if i.state == "done"]
     fin = sorted(i.finish_ms for i in done)
     span = max(fin[-1] - fin[0], 1e-3) / 1e3
@@ -560,6 +572,8 @@ def poisson_run(server, descs, rate, seconds, seed):
     return {"rate_qps": rate, "requests": n, "completed": len(done),
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "throughput_qps": tput,
+            "p50_first_third_ms": float(np.percentile(lat[:third], 50)),
+            "p50_last_third_ms": float(np.percentile(lat[-third:], 50)),
             "sustained": bool(tput >= 0.9 * rate)}
 
 
@@ -580,11 +594,17 @@ def run_serve(args):
                                            sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
                                            sssp_chunk_direction=args.sssp_chunk_direction,
                                            serve_admission=args.serve_admission,
+                                           serve_groups=args.serve_groups,
                                            profile_kernels=args.serve_profile)) as srv:
-        poisson_run(srv, descs[:64], 200, 0.3, seed=7)  # warm-up
+        outs = None
+        if args.serve_out == "device":
+            import torch
+            outs = [torch.empty(g.num_vertices, dtype=torch.int32, device="cuda")
+                    for _ in range(args.serve_out_ring)]
+        poisson_run(srv, descs[:64], 200, 0.3, seed=7, outs=outs)  # warm-up
         for i, rate in enumerate(float(r) for r in args.serve_rates.split(",")):
             s0 = srv.stats()
-            row = poisson_run(srv, descs, rate, args.serve_seconds, seed=100 + i)
+            row = poisson_run(srv, descs, rate, args.serve_seconds, seed=100 + i, outs=outs)
             s1 = srv.stats()
             row["levels"] = s1["levels"] - s0["levels"]
             row["level_ms"] = (s1["busy_ms"] - s0["busy_ms"]) / max(1, row["levels"])
@@ -607,6 +627,9 @@ def run_serve(args):
             "sssp_pull_edge_ratio": args.sssp_pull_edge_ratio,
             "admission": {"slots": "any free slot", "chunks": "whole 32-slot cohorts",
                           "group": "group cohorts"}[args.serve_admission],
+            "groups": args.serve_groups or 1,
+            "results": ({"device": f"written to a ring of {args.serve_out_ring} device buffers",
+                         "none": "discarded"})[args.serve_out],
             "seconds_per_rate": args.serve_seconds, "rates": rows, "graph_gen_s": gen_s}
     print(json.dumps(line), flush=True)
     if args.json_out:

@@ -301,6 +301,7 @@ class RunOptions:
     bfs_pull_chunks: bool = False  # CTA-chunked light-vertex BFS pull on levels that read most edges
     serve_admission: str = "slots"  # serving: "slots" (any free slot), "chunks" (whole 32-slot
                                     # cohorts) or "group" (a new cohort only in an empty group)
+    serve_groups: int = 0  # serving: traversal groups, each on its own stream (0 = 1)
     stream: int = 0
 
     def to_c(self) -> N.CgpOptions:
@@ -333,6 +334,9 @@ class RunOptions:
         if self.serve_admission not in ("slots", "chunks", "group"):
             raise ValueError("serve_admission must be slots, chunks or group")
         o.serve_admission = {"slots": 0, "chunks": 1, "group": 2}[self.serve_admission]
+        if not 0 <= self.serve_groups <= 8:
+            raise ValueError("serve_groups must be in [0, 8]")
+        o.serve_groups = int(self.serve_groups)
         o.stream = self.stream or None
         return o
 

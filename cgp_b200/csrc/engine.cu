@@ -348,7 +348,7 @@ struct LevelLaunch {
   bool pull;
   bool spull;        // SSSP gather kernels are part of the level
   bool gvec;         // rows allow the vectorised gather (alignment, width)
-  bool lchunks;      // light vertices gathered in CTA chunks (W <= 4)
+  bool lchunks;      // light vertices gathered in CTA chunks (in 4-word slices above W = 4)
   int dense_unroll;  // edges per step of the dense SSSP kernel (1 or 2)
   KernelTimer* kt;   // per-class event timing (non-graph runs only)
   bool heavy_push = false;                // heavy-queue push kernels are part of a level
@@ -453,10 +453,13 @@ int enqueue_level_t(const LevelLaunch& L, cudaStream_t s) {
         } else {
           k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
         }
-      } else if (L.gvec)
+      } else if (L.gvec && L.lchunks) {
+        k_sssp_pull_chunked<4, OT, WK, W><<<dim3(L.gr.gather_chunked, W / 4), kBlock, 0, s>>>(L.g, L.G);
+      } else if (L.gvec) {
         k_sssp_pull_vec<W, OT, WK><<<L.gr.gather_vec, kBlock, 0, s>>>(L.g, L.G);
-      else
+      } else {
         k_sssp_pull<W, OT, WK><<<L.gr.gather, kBlock, 0, s>>>(L.g, L.G);
+      }
       ++n;
     }
 
@@ -481,7 +484,12 @@ Grids grids_t(int sms) {
   if (tile == 0) {
     bfs_chunked = occupancy_grid(k_bfs_pull_chunked<W, OT, DEPTH>, sms);
     bfs_mid = occupancy_grid(k_bfs_pull_mid<W, OT, DEPTH>, sms);
-    if constexpr (W <= 4) gather_chunked = occupancy_grid(k_sssp_pull_chunked<W, OT, WK>, sms);
+    if constexpr (W <= 4) {
+      gather_chunked = occupancy_grid(k_sssp_pull_chunked<W, OT, WK>, sms);
+    } else {
+      // slices of 4 words, all resident at once: x blocks per slice
+      gather_chunked = std::max(1, occupancy_grid(k_sssp_pull_chunked<4, OT, WK, W>, sms) / (W / 4));
+    }
     gather_vec = occupancy_grid(k_sssp_pull_vec<W, OT, WK>, sms);
     gather_heavy_vec = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK, (W <= 4 ? 1 : 0)>, sms);
     gather_heavy_vec2 = occupancy_grid(k_sssp_pull_heavy_vec<W, OT, WK, 2>, sms);
@@ -726,7 +734,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
     const int elem = spec.W == 1 ? 2 : 4;
     L.gvec = L.g.values != nullptr && spec.Qg % elem == 0 &&
              reinterpret_cast<uintptr_t>(L.g.values) % (4 * elem) == 0;
-    L.lchunks = spec.W <= 4 && o.light_chunks >= 0;
+    L.lchunks = o.light_chunks >= 0;
   }
   L.dense_unroll = o.dense_unroll == 2 ? 2 : 1;
   L.chunk_dir = L.spull && sssp_chunk_dir(spec, o);
@@ -894,6 +902,11 @@ void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options
       ck(cudaMemcpy(out->profiles.data(), ws->prof.p, n * sizeof(LevelProfile),
                     cudaMemcpyDeviceToHost), "read profiles");
   }
+}
+
+void group_enqueue_levels(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
+                          cudaStream_t s, int levels) {
+  spec.launches += enqueue_levels(g, ws, spec, o, s, levels, nullptr);
 }
 
 void group_write_output(GraphImpl* g, Workspace* ws, GroupSpec& spec, OutMap om,

@@ -202,6 +202,10 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
 // many levels.  With a KernelTimer, levels run one at a time without graphs.
 void group_enact(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
                  cudaStream_t s, GroupRun* out, int max_levels, KernelTimer* kt = nullptr);
+// Enqueues `levels` levels on stream s without waiting for them (the serving
+// loop overlaps several groups this way).
+void group_enqueue_levels(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_options& o,
+                          cudaStream_t s, int levels);
 void group_write_output(GraphImpl* g, Workspace* ws, GroupSpec& spec,
                         dev::OutMap om, int query_major, cudaStream_t s);
 int choose_words(int n, int requested);

@@ -1864,7 +1864,7 @@ __device__ __forceinline__ void relax_min_row(uint32_t (&best)[N], const uint32_
 // without gathering slots is never read); bit j of *slots: slot j of the lane
 // gathers.
 template <int W>
-__device__ __forceinline__ void gather_vec_masks(const LevelCtl* ctl, int Qg, int lane,
+__device__ __forceinline__ void gather_vec_masks(const uint64_t* gsel, int Qg, int lane,
                                                  uint32_t* parts, uint32_t* slots) {
   using GV = GatherVec<W>;
   uint32_t pm = 0, sm = 0;
@@ -1874,7 +1874,7 @@ __device__ __forceinline__ void gather_vec_masks(const LevelCtl* ctl, int Qg, in
 #pragma unroll
     for (int k = 0; k < GV::kElem; ++k) {
       const int q = base + k;
-      if (q < Qg && ((ctl->gsel[q >> 6] >> (q & 63)) & 1ULL)) sm |= 1u << (r * GV::kElem + k);
+      if (q < Qg && ((gsel[q >> 6] >> (q & 63)) & 1ULL)) sm |= 1u << (r * GV::kElem + k);
     }
     if (base < Qg && ((sm >> (r * GV::kElem)) & ((1u << GV::kElem) - 1u))) pm |= 1u << r;
   }
@@ -1903,11 +1903,16 @@ __device__ __forceinline__ void gather_vec_words(uint32_t bits, int lane,
 
 // 32-slot chunks that hold a gathering SSSP slot at this level.
 template <int W>
-__device__ __forceinline__ uint32_t gather_chunks(const LevelCtl* ctl) {
+__device__ __forceinline__ uint32_t gather_chunks(const uint64_t* gsel) {
   uint64_t gs[W];
 #pragma unroll
-  for (int i = 0; i < W; ++i) gs[i] = ctl->gsel[i];
+  for (int i = 0; i < W; ++i) gs[i] = gsel[i];
   return chunk_bits<W>(gs);
+}
+
+template <int W>
+__device__ __forceinline__ uint32_t gather_chunks(const LevelCtl* ctl) {
+  return gather_chunks<W>(ctl->gsel);
 }
 
 // Whether the gather screens in-edges by their source's frontier chunks (-1)
@@ -2096,7 +2101,7 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   const int wib = threadIdx.x >> 5;
   const uint64_t* sb = ctl->gsel;
   uint32_t pmask, smask;
-  gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
+  gather_vec_masks<W>(ctl->gsel, g.Qg, lane, &pmask, &smask);
   const unsigned long long gw = (static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nwarps = (static_cast<unsigned long long>(gridDim.x) * blockDim.x) >> 5;
   const size_t Qg = static_cast<size_t>(g.Qg);
@@ -2203,10 +2208,14 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
 // vertex into that vertex's row in shared memory, and after a barrier each
 // vertex is committed once (compare, store, frontier words, append: no
 // atomics, the chunk owns its vertices).  W <= 4 (a row of 64W slots fits
-// 32 times in 32 KB of shared memory).
-template <int W, typename OT, int WK>
+// 32 times in 32 KB of shared memory).  Wider groups (WF = 8 or 16 words)
+// are gathered in slices of W words: blockIdx.y is the slice, each CTA owns
+// its vertices' slice of the row, and the frontier append is claimed with an
+// atomic on the stamp (the slices of a vertex commit in different CTAs).
+template <int W, typename OT, int WK, int WF = W>
 __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, DevGraph G) {
   static_assert(W <= 4, "chunked gather holds 32 rows of at most 256 slots");
+  static_assert(WF % W == 0, "a group is a whole number of slices");
   using GV = GatherVec<W>;
   constexpr int E = GV::kElem;
   constexpr int P = GV::kParts;
@@ -2222,13 +2231,22 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
   __shared__ int32_t s_pre[kLightChunkVerts + 1];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const uint64_t* sb = ctl->gsel;
+  const int sl = WF > W ? static_cast<int>(blockIdx.y) : 0;  // slice of W words
+  const int s0 = sl * 64 * W;                                  // its first slot
+  const uint64_t* sb = ctl->gsel + sl * W;
   uint32_t pmask, smask;
-  gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
-  const int screen_qs = gather_screen_qs<W>(g, ctl, lv, G.E);
-  const uint32_t gch = gather_chunks<W>(ctl);
+  gather_vec_masks<W>(sb, g.Qg - s0, lane, &pmask, &smask);
+  const uint32_t gch = gather_chunks<W>(sb);
+  if (gch == 0) return;  // no gathering slot in this slice (uniform over the CTA)
+  // screen or read whole rows: one decision for the whole group
+  int screen_qs = gather_screen_qs<WF>(g, ctl, lv, G.E);
+  if (screen_qs >= 0) {
+    screen_qs = 0;
+#pragma unroll
+    for (int i = 0; i < W; ++i) screen_qs += __popcll(sb[i]);
+  }
   const size_t Qg = static_cast<size_t>(g.Qg);
-  const uint32_t* lanebase = g.values + lane * E;
+  const uint32_t* lanebase = g.values + s0 + lane * E;
   WarpAppender ap;
   uint32_t uacc = 0;
   unsigned long long improved = 0, pairs = 0;
@@ -2296,11 +2314,11 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
         u = G.pcol[e];
         wb = weight_bits<WK>(G.pw, e);
         if (screen_qs < 0 && g.fsum != nullptr) {
-          cm = summary_chunks(g.fsum, lv.level, u) & gch;
+          cm = (summary_chunks(g.fsum, lv.level, u) >> (2 * W * sl)) & gch;
           cnt = __popc(cm) << 5;
         } else if (screen_qs < 0) {
           uint64_t m[W];
-          load_mask<W>(lv.fcur + static_cast<size_t>(u) * W, m);
+          load_mask<W>(lv.fcur + static_cast<size_t>(u) * WF + sl * W, m);
           // the next batch's source masks move to L2 while this batch's rows load
           const int fn = f + 32;
           if (fn < fb) {
@@ -2310,7 +2328,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
               if (s_pre[mid] <= fn) a = mid;
               else b = mid - 1;
             }
-            prefetch_l2(lv.fcur + static_cast<size_t>(G.pcol[s_beg[a] + (fn - s_pre[a])]) * W);
+            prefetch_l2(lv.fcur + static_cast<size_t>(G.pcol[s_beg[a] + (fn - s_pre[a])]) * WF + sl * W);
           }
 #pragma unroll
           for (int i = 0; i < W; ++i) {
@@ -2321,7 +2339,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
         } else {
           cnt = screen_qs;
         }
-        ++scanned;
+        if (sl == 0) ++scanned;  // in-edges counted once per group
       }
       pairs += static_cast<unsigned long long>(cnt);
       const unsigned lm = __ballot_sync(kFull, cnt > 0);
@@ -2364,7 +2382,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
     // commit: warp wib takes vertices wib, wib + 8, ...
     for (int k = wib; k < nv; k += kWarpsPerBlock) {
       const int32_t v = s_v[k];
-      uint32_t* row = g.values + static_cast<size_t>(v) * Qg + lane * E;
+      uint32_t* row = g.values + static_cast<size_t>(v) * Qg + s0 + lane * E;
       const uint32_t* srow = s_best + k * R + lane * E;
       uint32_t imp = 0;
 #pragma unroll
@@ -2389,7 +2407,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
         if (bits) store_vec<E>(row + 32 * E * r, nvv);
         imp |= bits << (r * E);
       }
-      if (lane == 0) ++verts;
+      if (lane == 0 && sl == 0) ++verts;
       if (!__any_sync(kFull, imp != 0)) continue;
       improved += __popc(imp);
       uacc |= imp;
@@ -2399,12 +2417,19 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
       for (int r = 0; r < P; ++r) {
         if (words[r]) {
           const int wi = ((32 * r + lane) * E) >> 6;
-          lv.fnext[static_cast<size_t>(v) * W + wi] |= words[r];
+          lv.fnext[static_cast<size_t>(v) * WF + sl * W + wi] |= words[r];
         }
       }
-      const bool fresh = g.stamp[v] < lv.level + 1;  // uniform
-      __syncwarp();
-      if (fresh && lane == 0) g.stamp[v] = lv.level + 1;
+      bool fresh;
+      if constexpr (WF > W) {
+        int old = 0;
+        if (lane == 0) old = atomicMax(g.stamp + v, lv.level + 1);
+        fresh = __shfl_sync(kFull, old, 0) < lv.level + 1;
+      } else {
+        fresh = g.stamp[v] < lv.level + 1;  // uniform
+        __syncwarp();
+        if (fresh && lane == 0) g.stamp[v] = lv.level + 1;
+      }
       ap.add<OT>(fresh && lane == 0, v, G, lv, lane);
     }
     __syncthreads();
@@ -2415,7 +2440,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
     gather_vec_words<W>(uacc, lane, words);
 #pragma unroll
     for (int r = 0; r < P; ++r)
-      if (words[r]) atomic_or64(lv.nactive + (((32 * r + lane) * E) >> 6), words[r]);
+      if (words[r]) atomic_or64(lv.nactive + sl * W + (((32 * r + lane) * E) >> 6), words[r]);
   }
   warp_add(improved, &g.ctl->lc.improved, lane);
   warp_add(pairs, &g.ctl->lc.sssp_pairs, lane);
@@ -2445,7 +2470,7 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   const int wib = threadIdx.x >> 5;
   const uint64_t* sb = ctl->gsel;
   uint32_t pmask, smask;
-  gather_vec_masks<W>(ctl, g.Qg, lane, &pmask, &smask);
+  gather_vec_masks<W>(ctl->gsel, g.Qg, lane, &pmask, &smask);
   const uint32_t lsel = lane_sssp_chunks<W>(ctl, lane);
   const int screen_qs = gather_screen_qs<W>(g, ctl, lv, G.E);
   const uint32_t gch = gather_chunks<W>(ctl);

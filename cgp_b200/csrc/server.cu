@@ -1,4 +1,5 @@
-// Continuous-batching server over one traversal group of bitmask slots.
+// Continuous-batching server over one or more traversal groups of bitmask
+// slots.
 //
 // Replaces replenish_frontier_engine / run_replenish_pipeline
 // (puercgp/include/puercgp/engine/replenish_engine.hxx:42-573).  The
@@ -45,6 +46,7 @@ struct RetireReq {
   int32_t kind;
   int32_t has_out;
   int32_t reserved;
+  uint32_t* dst;  // the request's device output, or NULL: staging row i
 };
 
 // Seeds newly admitted slots into the frontier of the current level (one
@@ -116,11 +118,12 @@ __global__ void k_admit(GroupDev g, DevGraph G, const AdmitReq* reqs, int n) {
 }
 
 // Retires slots: snapshot each slot column (mapped to its kind's unreached
-// marker) into staging row i, reset the column, and clear the slots' visited
-// bits (and frontier bits when a running request was cancelled).  A CTA
-// takes 64 vertices: its warps read the retiring slots of one vertex row
-// together (lane i <-> slot i, all within the row's 1 KB), stage them in
-// shared memory, and then write every slot's staging row contiguously.
+// marker) into the request's device output, or staging row i for a host
+// output, reset the column, and clear the slots' visited bits (and frontier
+// bits when a running request was cancelled).  A CTA takes 64 vertices: its
+// warps read the retiring slots of one vertex row together (lane i <-> slot
+// i, all within the row's 1 KB), stage them in shared memory, and then write
+// every slot's output row contiguously.
 constexpr int kRetireTile = 64;
 
 template <int W>
@@ -174,7 +177,10 @@ __global__ void __launch_bounds__(kBlock) k_retire(GroupDev g, int64_t V, const 
     if (any_out) {
       for (int t = threadIdx.x; t < n * kRetireTile; t += blockDim.x) {
         const int i = t / kRetireTile, j = t % kRetireTile;
-        if (rq[i].has_out && v0 + j < V) staging[static_cast<size_t>(i) * V + v0 + j] = tile[i][j];
+        if (rq[i].has_out && v0 + j < V) {
+          uint32_t* row = rq[i].dst ? rq[i].dst : staging + static_cast<size_t>(i) * V;
+          row[v0 + j] = tile[i][j];
+        }
       }
     }
     __syncthreads();
@@ -210,21 +216,42 @@ struct Request {
 using namespace cgp;
 using namespace cgp::dev;
 
-struct cgp_server {
-  GraphImpl* g = nullptr;
-  cgp_options o{};
-  int S = 0;
-  int W = 1;
+// One traversal group of the server: its own workspace (masks, values,
+// control block), stream and admission buffers.  Slots of group g are the
+// global slots [base, base + S).
+struct ServeGroup {
   std::unique_ptr<Workspace> ws;
   GroupSpec spec;
   cudaStream_t stream = nullptr;
+  int S = 0;
+  int W = 1;
+  int base = 0;
+  int active = 0;        // occupied slots
+  bool cohort = false;   // group-cohort policy: a cohort runs here (no admissions)
+  int32_t level = 0;     // device level at the last read
+  int64_t levels_done = 0;
+  int64_t sssp_chunk_levels = 0, gather_chunk_levels = 0;
+  DevBuf admit_dev, retire_dev, clear_dev;
+  AdmitReq* h_admit = nullptr;
+  RetireReq* h_retire = nullptr;
+  uint64_t* h_clear = nullptr;
+  int32_t* h_level = nullptr;
+  int nadmit = 0;        // admissions of the current pass
+  bool ran = false;      // levels were enqueued in the current pass
+};
+
+struct cgp_server {
+  GraphImpl* g = nullptr;
+  cgp_options o{};
+  int S = 0;             // total slots over all groups
+  std::vector<ServeGroup> groups;
   std::thread th;
   std::mutex mu;
   std::condition_variable cv;       // work arrived / stop
   std::condition_variable done_cv;  // a request finished
   std::deque<uint64_t> pending;
   std::unordered_map<uint64_t, Request> reqs;
-  std::vector<int64_t> slot_ticket;
+  std::vector<int64_t> slot_ticket;  // by global slot
   int active = 0;
   bool stop = false;
   uint64_t next_ticket = 1;
@@ -239,10 +266,8 @@ struct cgp_server {
   int64_t state_bytes = 0;
   bool wcc_ready = false;
   std::string fatal;
-  DevBuf admit_dev, retire_dev, clear_dev, staging;
-  AdmitReq* h_admit = nullptr;
-  RetireReq* h_retire = nullptr;
-  uint64_t* h_clear = nullptr;
+  DevBuf staging;        // retire snapshots (groups retire one after another)
+  std::unique_ptr<Workspace> wcc_ws;  // WCC labels
   std::unique_ptr<KernelTimer> kt;  // per-class kernel times (profile_kernels)
   std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
 
@@ -250,9 +275,10 @@ struct cgp_server {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   void loop();
-  int pick_slot();
+  int pick_slot(int* group);
   void finish_wcc(std::vector<uint64_t>& tickets);
-  void retire(std::vector<int>& slots_to_retire, bool forced);
+  void retire(ServeGroup& gr, std::vector<int>& local_slots, bool forced);
+  void release_pinned();
 };
 
 namespace {
@@ -286,9 +312,9 @@ RetireFn pick_retire(int W) {
   }
 }
 
-GroupDev server_dev(cgp_server* sv) {
+GroupDev server_dev(const ServeGroup& gr) {
   GroupDev g{};
-  Workspace* ws = sv->ws.get();
+  Workspace* ws = gr.ws.get();
   g.visited = ws->visited.as<uint64_t>();
   g.fbuf0 = ws->fbuf0.as<uint64_t>();
   g.fbuf1 = ws->fbuf1.as<uint64_t>();
@@ -305,17 +331,32 @@ GroupDev server_dev(cgp_server* sv) {
   g.ctl = ws->ctl.as<LevelCtl>();
   g.prof = nullptr;
   g.slots = ws->slots.as<SlotDev>();
-  g.Qg = sv->S;
+  g.Qg = gr.S;
   return g;
 }
 
 }  // namespace
 
+void cgp_server::release_pinned() {
+  for (ServeGroup& gr : groups) {
+    if (gr.stream) cudaStreamSynchronize(gr.stream);
+    if (gr.h_admit) cudaFreeHost(gr.h_admit);
+    if (gr.h_retire) cudaFreeHost(gr.h_retire);
+    if (gr.h_clear) cudaFreeHost(gr.h_clear);
+    if (gr.h_level) cudaFreeHost(gr.h_level);
+    gr.h_admit = nullptr;
+    gr.h_retire = nullptr;
+    gr.h_clear = nullptr;
+    gr.h_level = nullptr;
+  }
+}
+
 void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
   if (tickets.empty()) return;
+  cudaStream_t s = wcc_ws->stream;
   if (!wcc_ready) {
-    ws->wcc.ensure(static_cast<size_t>(g->V) * 4);
-    wcc_labels(g, ws->wcc.as<uint32_t>(), stream);
+    wcc_ws->wcc.ensure(static_cast<size_t>(g->V) * 4);
+    wcc_labels(g, wcc_ws->wcc.as<uint32_t>(), s);
     wcc_ready = true;
   }
   std::vector<std::pair<void*, bool>> outs;
@@ -325,10 +366,10 @@ void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
   }
   for (auto& o : outs)
     if (o.first)
-      ck(cudaMemcpyAsync(o.first, ws->wcc.p, static_cast<size_t>(g->V) * 4,
-                         o.second ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream),
+      ck(cudaMemcpyAsync(o.first, wcc_ws->wcc.p, static_cast<size_t>(g->V) * 4,
+                         o.second ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s),
          "wcc result");
-  ck(cudaStreamSynchronize(stream), "wcc");
+  ck(cudaStreamSynchronize(s), "wcc");
   std::lock_guard<std::mutex> lk(mu);
   const double t = now_ms();
   for (uint64_t tk : tickets) {
@@ -342,101 +383,56 @@ void cgp_server::finish_wcc(std::vector<uint64_t>& tickets) {
   done_cv.notify_all();
 }
 
-// A free slot for the next admission (mu held), or -1.  Slots are taken in
-// 32-slot cohorts, so that requests that arrive together share a chunk and
-// pass through their sparse and dense phases together (what the per-chunk
-// SSSP direction needs): first a chunk already taken by this admission pass,
-// then an empty chunk, then the chunk whose occupants were admitted last.
-// (Separating SSSP from BFS-like requests into chunks of their own was
-// measured too: lower capacity on R-MAT 24, 329 against 380 q/s at 500 q/s
-// offered, since a saturated server refills single freed slots and an
-// all-SSSP chunk then gathers at most levels.)
-int cgp_server::pick_slot() {
-  // group cohorts: a new cohort starts only in an empty group (the requests
-  // of this admission pass join it); then every gather level of the group is
-  // shared by all its SSSP requests
-  if (o.serve_admission == 2) {
-    for (int i = 0; i < S; ++i)
-      if (slot_ticket[i] >= 0 && reqs[static_cast<uint64_t>(slot_ticket[i])].admit_level >= 0)
-        return -1;
-  }
-  int best = -1;
-  long long best_key = -1;
-  for (int c0 = 0; c0 < S; c0 += 32) {
-    const int c1 = std::min(S, c0 + 32);
-    int free_slot = -1, occupied = 0, newest = -1;
-    bool this_pass = false;
-    for (int i = c0; i < c1; ++i) {
-      if (slot_ticket[i] < 0) {
-        if (free_slot < 0) free_slot = i;
-        continue;
-      }
-      ++occupied;
-      const int al = reqs[static_cast<uint64_t>(slot_ticket[i])].admit_level;
-      if (al < 0) this_pass = true;  // level set once the admission kernel ran
-      newest = std::max(newest, al);
-    }
-    if (free_slot < 0) continue;
-    // whole cohorts: a chunk with occupants from earlier passes takes no one
-    if (o.serve_admission == 1 && occupied > 0 && !this_pass) continue;
-    const long long key = this_pass ? (3LL << 40) : occupied == 0 ? (2LL << 40) : newest;
-    if (key > best_key) {
-      best_key = key;
-      best = free_slot;
-    }
-  }
-  return best;
-}
-
-void cgp_server::retire(std::vector<int>& to_retire, bool forced) {
+// Retires local slots of group gr: snapshots their columns into the staging
+// rows, resets them, copies the results out, in passes of kRetireBatch.
+void cgp_server::retire(ServeGroup& gr, std::vector<int>& to_retire, bool forced) {
   const double t_start = now_ms();
   const int64_t V = g->V;
   const uint32_t f32 = g->weight_kind == CGP_WEIGHT_F32 ? 1u : 0u;
-  RetireFn rf = pick_retire(W);
+  RetireFn rf = pick_retire(gr.W);
   for (size_t b = 0; b < to_retire.size(); b += kRetireBatch) {
     const int n = static_cast<int>(std::min<size_t>(kRetireBatch, to_retire.size() - b));
-    std::memset(h_clear, 0, kMaxWords * 8);
+    std::memset(gr.h_clear, 0, kMaxWords * 8);
     std::vector<uint64_t> tickets(n);
     std::vector<std::pair<void*, bool>> outs(n);
     {
       std::lock_guard<std::mutex> lk(mu);
       for (int i = 0; i < n; ++i) {
         const int s = to_retire[b + i];
-        tickets[i] = static_cast<uint64_t>(slot_ticket[s]);
+        tickets[i] = static_cast<uint64_t>(slot_ticket[gr.base + s]);
         Request& r = reqs[tickets[i]];
         outs[i] = {r.out, r.out_dev};
-        h_retire[i].slot = s;
-        h_retire[i].kind = r.q.kind;
-        h_retire[i].has_out = (r.out != nullptr && !r.cancel) ? 1 : 0;
-        h_clear[s >> 6] |= 1ULL << (s & 63);
+        gr.h_retire[i].slot = s;
+        gr.h_retire[i].kind = r.q.kind;
+        gr.h_retire[i].has_out = (r.out != nullptr && !r.cancel) ? 1 : 0;
+        // device outputs are written by the retire kernel itself
+        gr.h_retire[i].dst = r.out_dev ? static_cast<uint32_t*>(r.out) : nullptr;
+        gr.h_clear[s >> 6] |= 1ULL << (s & 63);
       }
     }
-    ck(cudaMemcpyAsync(retire_dev.p, h_retire, n * sizeof(RetireReq), cudaMemcpyHostToDevice, stream),
-       "upload retire");
-    ck(cudaMemcpyAsync(clear_dev.p, h_clear, kMaxWords * 8, cudaMemcpyHostToDevice, stream),
+    ck(cudaMemcpyAsync(gr.retire_dev.p, gr.h_retire, n * sizeof(RetireReq), cudaMemcpyHostToDevice,
+                       gr.stream), "upload retire");
+    ck(cudaMemcpyAsync(gr.clear_dev.p, gr.h_clear, kMaxWords * 8, cudaMemcpyHostToDevice, gr.stream),
        "upload clear");
-    rf(server_dev(this), V, retire_dev.as<RetireReq>(), n, staging.as<uint32_t>(),
-       clear_dev.as<uint64_t>(), forced ? 1 : 0, f32, g->num_sms * 4, stream);
+    rf(server_dev(gr), V, gr.retire_dev.as<RetireReq>(), n, staging.as<uint32_t>(),
+       gr.clear_dev.as<uint64_t>(), forced ? 1 : 0, f32, g->num_sms * 4, gr.stream);
     ck(cudaGetLastError(), "retire");
     for (int i = 0; i < n; ++i) {
-      if (h_retire[i].has_out)
+      if (gr.h_retire[i].has_out && !outs[i].second)
         ck(cudaMemcpyAsync(outs[i].first, staging.as<uint32_t>() + static_cast<size_t>(i) * V,
-                           static_cast<size_t>(V) * 4,
-                           outs[i].second ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                           stream),
+                           static_cast<size_t>(V) * 4, cudaMemcpyDeviceToHost, gr.stream),
            "result copy");
     }
-    ck(cudaStreamSynchronize(stream), "retire");
-    LevelCtl c;
-    ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
+    ck(cudaStreamSynchronize(gr.stream), "retire");
     std::lock_guard<std::mutex> lk(mu);
     const double t = now_ms();
     for (int i = 0; i < n; ++i) {
       Request& r = reqs[tickets[i]];
       r.state = r.cancel ? 3 : 2;
       r.t_finish = t;
-      r.completion_level = c.level - r.admit_level;
-      slot_ticket[h_retire[i].slot] = -1;
+      r.completion_level = gr.level - r.admit_level;
+      slot_ticket[gr.base + gr.h_retire[i].slot] = -1;
+      --gr.active;
       --active;
       ++completed;
     }
@@ -446,19 +442,72 @@ void cgp_server::retire(std::vector<int>& to_retire, bool forced) {
   retire_ms += now_ms() - t_start;
 }
 
+// A free global slot for the next admission (mu held), or -1; *group gets
+// its group.  Slots are taken in 32-slot cohorts, so that requests that
+// arrive together share a chunk and pass through their sparse and dense
+// phases together (what the per-chunk SSSP direction needs): first a chunk
+// already taken by this admission pass, then an empty chunk, then the chunk
+// whose occupants were admitted last.  Policies (cgp_options.serve_admission):
+//  * 0, free slots: any free slot, in that order of preference.
+//  * 1, chunk cohorts: a chunk with occupants from earlier passes takes no one.
+//  * 2, group cohorts: a group takes requests only while it is empty or
+//    filling in this pass, so each group runs one cohort at a time and every
+//    gather level of the group serves all of its SSSP requests; with two or
+//    more groups, arrivals open a cohort in an idle group while the others
+//    run, and the groups' levels overlap on the device.
+// (Separating SSSP from BFS-like requests into chunks of their own was
+// measured too: lower capacity on R-MAT 24, 329 against 380 q/s at 500 q/s
+// offered, since a saturated server refills single freed slots and an
+// all-SSSP chunk then gathers at most levels.)
+int cgp_server::pick_slot(int* group) {
+  const int pol = o.serve_admission;
+  int best = -1, best_g = -1;
+  long long best_key = -1;
+  for (int gi = 0; gi < static_cast<int>(groups.size()); ++gi) {
+    ServeGroup& gr = groups[gi];
+    if (pol == 2 && gr.cohort && gr.nadmit == 0) continue;  // a cohort runs here
+    for (int c0 = 0; c0 < gr.S; c0 += 32) {
+      const int c1 = std::min(gr.S, c0 + 32);
+      int free_slot = -1, occupied = 0, newest = -1;
+      bool this_pass = false;
+      for (int i = c0; i < c1; ++i) {
+        const int64_t t = slot_ticket[gr.base + i];
+        if (t < 0) {
+          if (free_slot < 0) free_slot = i;
+          continue;
+        }
+        ++occupied;
+        const int al = reqs[static_cast<uint64_t>(t)].admit_level;
+        if (al < 0) this_pass = true;  // level set once the admission kernel ran
+        newest = std::max(newest, al);
+      }
+      if (free_slot < 0) continue;
+      if (pol == 1 && occupied > 0 && !this_pass) continue;
+      long long key = this_pass ? (3LL << 40) : occupied == 0 ? (2LL << 40) : newest;
+      if (pol == 2 && gr.nadmit > 0) key += 4LL << 40;  // one cohort per pass stays together
+      if (key > best_key) {
+        best_key = key;
+        best = gr.base + free_slot;
+        best_g = gi;
+      }
+    }
+  }
+  *group = best_g;
+  return best;
+}
+
 void cgp_server::loop() {
   try {
     ck(cudaSetDevice(g->device), "cudaSetDevice");
-    AdmitFn af = pick_admit(W, g->offset_bytes);
     const int per = o.levels_per_sync > 0 ? o.levels_per_sync : 2;
     for (;;) {
       std::vector<uint64_t> wcc_tickets;
-      int nadmit = 0;
       {
         std::unique_lock<std::mutex> lk(mu);
         cv.wait_for(lk, std::chrono::milliseconds(50),
                     [&] { return stop || !pending.empty() || active > 0; });
         if (stop) break;
+        for (ServeGroup& gr : groups) gr.nadmit = 0;
         const double t = now_ms();
         while (!pending.empty()) {
           const uint64_t tk = pending.front();
@@ -477,68 +526,119 @@ void cgp_server::loop() {
             wcc_tickets.push_back(tk);
             continue;
           }
-          const int s = pick_slot();
+          int gi = -1;
+          const int s = pick_slot(&gi);
           if (s < 0) break;
+          ServeGroup& gr = groups[gi];
           pending.pop_front();
           slot_ticket[s] = static_cast<int64_t>(tk);
+          ++gr.active;
           ++active;
           r.state = 1;
           r.slot = s;
           r.t_admit = t;
-          h_admit[nadmit].slot = s;
-          h_admit[nadmit].kind = r.q.kind;
-          h_admit[nadmit].source = r.q.source;
-          h_admit[nadmit].k = r.q.k;
-          ++nadmit;
+          AdmitReq& a = gr.h_admit[gr.nadmit++];
+          a.slot = s - gr.base;
+          a.kind = r.q.kind;
+          a.source = r.q.source;
+          a.k = r.q.k;
         }
       }
       finish_wcc(wcc_tickets);
-      if (nadmit > 0) {
-        const double ta = now_ms();
-        LevelCtl c;
-        ck(cudaMemcpyAsync(&c.level, reinterpret_cast<char*>(ws->ctl.p) + offsetof(LevelCtl, level),
-                           sizeof(int32_t), cudaMemcpyDeviceToHost, stream), "read level");
-        ck(cudaMemcpyAsync(admit_dev.p, h_admit, nadmit * sizeof(AdmitReq), cudaMemcpyHostToDevice,
-                           stream), "upload admits");
-        af(server_dev(this), g->dev_graph(heavy_threshold(o)), admit_dev.as<AdmitReq>(), nadmit,
-           stream);
+      const double ta = now_ms();
+      bool admitted = false;
+      for (ServeGroup& gr : groups) {
+        if (gr.nadmit == 0) continue;
+        admitted = true;
+        ck(cudaMemcpyAsync(gr.h_level, reinterpret_cast<char*>(gr.ws->ctl.p) + offsetof(LevelCtl, level),
+                           sizeof(int32_t), cudaMemcpyDeviceToHost, gr.stream), "read level");
+        ck(cudaMemcpyAsync(gr.admit_dev.p, gr.h_admit, gr.nadmit * sizeof(AdmitReq),
+                           cudaMemcpyHostToDevice, gr.stream), "upload admits");
+        pick_admit(gr.W, g->offset_bytes)(server_dev(gr), g->dev_graph(heavy_threshold(o)),
+                                          gr.admit_dev.as<AdmitReq>(), gr.nadmit, gr.stream);
         ck(cudaGetLastError(), "admit");
-        ck(cudaStreamSynchronize(stream), "admit");
+      }
+      if (admitted) {
+        for (ServeGroup& gr : groups)
+          if (gr.nadmit > 0) ck(cudaStreamSynchronize(gr.stream), "admit");
         std::lock_guard<std::mutex> lk(mu);
-        for (int i = 0; i < nadmit; ++i) reqs[slot_ticket[h_admit[i].slot]].admit_level = c.level;
+        for (ServeGroup& gr : groups) {
+          if (gr.nadmit == 0) continue;
+          for (int i = 0; i < gr.nadmit; ++i)
+            reqs[static_cast<uint64_t>(slot_ticket[gr.base + gr.h_admit[i].slot])].admit_level =
+                *gr.h_level;
+          gr.cohort = true;
+        }
         admit_ms += now_ms() - ta;
       }
-      int act;
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        act = active;
-      }
-      if (act == 0) continue;
       const double tb = now_ms();
-      GroupRun r;
-      group_enact(g, ws.get(), spec, o, stream, &r, per, kt.get());
-      if (kt) kt->flush();
-      LevelCtl c;
-      ck(cudaMemcpy(&c, ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost), "read ctl");
-      busy_ms += now_ms() - tb;
-      levels = c.level;
-      sssp_chunk_levels = static_cast<int64_t>(c.sssp_chunk_levels);
-      gather_chunk_levels = static_cast<int64_t>(c.gather_chunk_levels);
-      // converged: occupied, admitted before the current level, no frontier bit
-      std::vector<int> conv, forced;
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        const uint64_t* act_bits = c.active[c.level & 1];
-        for (int s = 0; s < S; ++s) {
-          if (slot_ticket[s] < 0) continue;
-          Request& q = reqs[static_cast<uint64_t>(slot_ticket[s])];
-          const bool live = c.done != 1 && ((act_bits[s >> 6] >> (s & 63)) & 1ULL);
-          if (q.cancel) forced.push_back(s);
-          else if (q.admit_level < c.level && !live) conv.push_back(s);
+      // levels: every group with requests runs `per` levels; without kernel
+      // timing the groups' level chunks are enqueued on their own streams
+      // first and waited for afterwards, so they overlap on the device
+      bool any = false;
+      for (ServeGroup& gr : groups) {
+        gr.ran = false;
+        int act;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          act = gr.active;
         }
+        if (act == 0) {
+          gr.cohort = false;
+          continue;
+        }
+        gr.ran = true;
+        any = true;
+        if (kt) {
+          GroupRun r;
+          group_enact(g, gr.ws.get(), gr.spec, o, gr.stream, &r, per, kt.get());
+          kt->flush();
+        } else {
+          group_enqueue_levels(g, gr.ws.get(), gr.spec, o, gr.stream, per);
+        }
+        ck(cudaMemcpyAsync(gr.ws->hctl, gr.ws->ctl.p, sizeof(LevelCtl), cudaMemcpyDeviceToHost,
+                           gr.stream), "read ctl");
       }
-      if (!conv.empty()) retire(conv, false);
-      if (!forced.empty()) retire(forced, true);
+      if (!any) continue;
+      for (ServeGroup& gr : groups)
+        if (gr.ran) ck(cudaStreamSynchronize(gr.stream), "levels");
+      busy_ms += now_ms() - tb;
+      for (ServeGroup& gr : groups) {
+        if (!gr.ran) continue;
+        const LevelCtl& c = gr.ws->hctl[0];
+        if (c.status & kStatusQueueOverflow)
+          throw ApiError{CGP_ERR_DEVICE, "heavy frontier queue overflow"};
+        gr.level = c.level;
+        gr.levels_done = c.level;
+        gr.sssp_chunk_levels = static_cast<int64_t>(c.sssp_chunk_levels);
+        gr.gather_chunk_levels = static_cast<int64_t>(c.gather_chunk_levels);
+        // converged: occupied, admitted before the current level, no frontier bit
+        std::vector<int> conv, forced;
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          const uint64_t* act_bits = c.active[c.level & 1];
+          for (int s = 0; s < gr.S; ++s) {
+            const int64_t t = slot_ticket[gr.base + s];
+            if (t < 0) continue;
+            Request& q = reqs[static_cast<uint64_t>(t)];
+            const bool live = c.done != 1 && ((act_bits[s >> 6] >> (s & 63)) & 1ULL);
+            if (q.cancel) forced.push_back(s);
+            else if (q.admit_level < c.level && !live) conv.push_back(s);
+          }
+          levels = 0;
+          sssp_chunk_levels = 0;
+          gather_chunk_levels = 0;
+          for (const ServeGroup& x : groups) {
+            levels += x.levels_done;
+            sssp_chunk_levels += x.sssp_chunk_levels;
+            gather_chunk_levels += x.gather_chunk_levels;
+          }
+        }
+        if (!conv.empty()) retire(gr, conv, false);
+        if (!forced.empty()) retire(gr, forced, true);
+        std::lock_guard<std::mutex> lk(mu);
+        if (gr.active == 0) gr.cohort = false;
+      }
     }
   } catch (...) {
     cgp_status st = translate_exception();
@@ -565,6 +665,10 @@ cgp_status cgp_server_create(cgp_graph* graph, int32_t slots, const cgp_options*
   if (graph == nullptr) return set_error(CGP_ERR_INVALID_ARG, "graph is NULL");
   if (slots <= 0 || slots > kMaxWords * 64)
     return set_error(CGP_ERR_INVALID_ARG, "slots must be in [1, 1024]");
+  if (opts && (opts->serve_admission < 0 || opts->serve_admission > 2))
+    return set_error(CGP_ERR_INVALID_ARG, "serve_admission must be 0, 1 or 2");
+  if (opts && (opts->serve_groups < 0 || opts->serve_groups > 8))
+    return set_error(CGP_ERR_INVALID_ARG, "serve_groups must be in [0, 8]");
   auto* sv = new (std::nothrow) cgp_server();
   if (!sv) return set_error(CGP_ERR_OOM, "host allocation failed");
   try {
@@ -575,55 +679,75 @@ cgp_status cgp_server_create(cgp_graph* graph, int32_t slots, const cgp_options*
     else cgp_options_init(&sv->o);
     sv->o.profile_iterations = 0;
     sv->o.max_iterations = 0;
+    // groups: one unless asked (on R-MAT 24 serving, one 256-slot group of
+    // cohorts sustained 500 q/s at p99 0.66 s; two groups of 128 or 256 slots
+    // gave 0.96 / 1.09 s: two cohorts at a time share every level's per-edge
+    // cost); never more groups than slots
+    int G = sv->o.serve_groups > 0 ? sv->o.serve_groups : 1;
+    G = std::max(1, std::min(G, static_cast<int>(slots)));
     // admission by device memory: slot width x |V| for the values, plus the
-    // per-vertex masks that every slot shares
+    // per-vertex masks of each group, plus the retire staging rows
     size_t free_b = 0, total_b = 0;
     ck(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
     const int64_t budget = max_state_bytes > 0 ? max_state_bytes
                                                : static_cast<int64_t>(0.8 * static_cast<double>(free_b));
-    int S = slots;
-    while (S > 1 && group_state_bytes(g, choose_words(S, sv->o.mask_words), S, kDepthDirect) +
-                        static_cast<int64_t>(kRetireBatch) * g->V * 4 > budget)
-      --S;
-    const int64_t need = group_state_bytes(g, choose_words(S, sv->o.mask_words), S, kDepthDirect) +
-                         static_cast<int64_t>(kRetireBatch) * g->V * 4;
+    auto need_for = [&](int total) {
+      int64_t b = static_cast<int64_t>(kRetireBatch) * g->V * 4;
+      for (int i = 0; i < G; ++i) {
+        const int Sg = total / G + (i < total % G ? 1 : 0);
+        if (Sg > 0) b += group_state_bytes(g, choose_words(Sg, sv->o.mask_words), Sg, kDepthDirect);
+      }
+      return b;
+    };
+    int S = std::max(slots, G);
+    while (S > G && need_for(S) > budget) --S;
+    if (S < G) S = G;
+    const int64_t need = need_for(S);
     if (need > budget) throw ApiError{CGP_ERR_OOM, "not enough device memory for one slot"};
     sv->S = S;
-    sv->W = choose_words(S, sv->o.mask_words);
     sv->state_bytes = need;
-    sv->ws = std::make_unique<Workspace>(g->device);
-    sv->stream = sv->ws->stream;
-    sv->spec.W = sv->W;
-    sv->spec.Qg = S;
-    sv->spec.slots.assign(S, SlotDev{-1, -1, 0, 0});
-    sv->spec.depth_mode = kDepthDirect;
-    sv->spec.has_bfs = true;
-    sv->spec.has_sssp = true;
-    sv->spec.uniform_inf = kServeInf;
-    sv->spec.serving = true;
-    group_prepare(g, sv->ws.get(), sv->spec, sv->o, sv->stream);
     sv->slot_ticket.assign(S, -1);
-    sv->admit_dev.ensure(kMaxWords * 64 * sizeof(AdmitReq));
-    sv->retire_dev.ensure(kRetireBatch * sizeof(RetireReq));
-    sv->clear_dev.ensure(kMaxWords * 8);
+    sv->groups.resize(G);
+    int base = 0;
+    for (int i = 0; i < G; ++i) {
+      ServeGroup& gr = sv->groups[i];
+      gr.S = S / G + (i < S % G ? 1 : 0);
+      gr.base = base;
+      base += gr.S;
+      gr.W = choose_words(gr.S, sv->o.mask_words);
+      gr.ws = std::make_unique<Workspace>(g->device);
+      gr.stream = gr.ws->stream;
+      gr.spec.W = gr.W;
+      gr.spec.Qg = gr.S;
+      gr.spec.slots.assign(gr.S, SlotDev{-1, -1, 0, 0});
+      gr.spec.depth_mode = kDepthDirect;
+      gr.spec.has_bfs = true;
+      gr.spec.has_sssp = true;
+      gr.spec.uniform_inf = kServeInf;
+      gr.spec.serving = true;
+      group_prepare(g, gr.ws.get(), gr.spec, sv->o, gr.stream);
+      gr.admit_dev.ensure(kMaxWords * 64 * sizeof(AdmitReq));
+      gr.retire_dev.ensure(kRetireBatch * sizeof(RetireReq));
+      gr.clear_dev.ensure(kMaxWords * 8);
+      ck(cudaHostAlloc(reinterpret_cast<void**>(&gr.h_admit), kMaxWords * 64 * sizeof(AdmitReq),
+                       cudaHostAllocDefault), "pinned");
+      ck(cudaHostAlloc(reinterpret_cast<void**>(&gr.h_retire), kRetireBatch * sizeof(RetireReq),
+                       cudaHostAllocDefault), "pinned");
+      ck(cudaHostAlloc(reinterpret_cast<void**>(&gr.h_clear), kMaxWords * 8, cudaHostAllocDefault),
+         "pinned");
+      ck(cudaHostAlloc(reinterpret_cast<void**>(&gr.h_level), sizeof(int32_t), cudaHostAllocDefault),
+         "pinned");
+    }
     sv->staging.ensure(static_cast<size_t>(kRetireBatch) * g->V * 4);
-    ck(cudaHostAlloc(reinterpret_cast<void**>(&sv->h_admit), kMaxWords * 64 * sizeof(AdmitReq),
-                     cudaHostAllocDefault), "pinned");
-    ck(cudaHostAlloc(reinterpret_cast<void**>(&sv->h_retire), kRetireBatch * sizeof(RetireReq),
-                     cudaHostAllocDefault), "pinned");
-    ck(cudaHostAlloc(reinterpret_cast<void**>(&sv->h_clear), kMaxWords * 8, cudaHostAllocDefault),
-       "pinned");
-    ck(cudaStreamSynchronize(sv->stream), "server init");
+    sv->wcc_ws = std::make_unique<Workspace>(g->device);
+    for (ServeGroup& gr : sv->groups) ck(cudaStreamSynchronize(gr.stream), "server init");
     if (sv->o.profile_kernels) sv->kt = std::make_unique<KernelTimer>();
     sv->th = std::thread([sv] { sv->loop(); });
     *out = sv;
     return CGP_OK;
   } catch (...) {
     cgp_status st = translate_exception();
-    if (sv->stream) cudaStreamSynchronize(sv->stream);
-    if (sv->h_admit) cudaFreeHost(sv->h_admit);
-    if (sv->h_retire) cudaFreeHost(sv->h_retire);
-    if (sv->h_clear) cudaFreeHost(sv->h_clear);
+    sv->release_pinned();
     delete sv;
     return st;
   }
@@ -638,10 +762,7 @@ cgp_status cgp_server_destroy(cgp_server* sv) {
   }
   sv->cv.notify_all();
   if (sv->th.joinable()) sv->th.join();
-  if (sv->stream) cudaStreamSynchronize(sv->stream);
-  if (sv->h_admit) cudaFreeHost(sv->h_admit);
-  if (sv->h_retire) cudaFreeHost(sv->h_retire);
-  if (sv->h_clear) cudaFreeHost(sv->h_clear);
+  sv->release_pinned();
   delete sv;
   return CGP_OK;
 }

@@ -108,8 +108,8 @@ typedef struct {
   int32_t dense_unroll;       /* edges per step of the dense SSSP kernel: 1 or 2; 0 = 1 */
   double sssp_pull_edge_ratio; /* SSSP levels gather (pull) when frontier edges >= ratio * E;
                                   <= 0: always scatter (push)                              */
-  int32_t light_chunks;       /* SSSP gathers take light vertices in CTA chunks (groups of up
-                                 to 256 slots): 0 = on, -1 = one warp per vertex           */
+  int32_t light_chunks;       /* SSSP gathers take light vertices in CTA chunks (wider groups
+                                 in 256-slot slices): 0 = on, -1 = one warp per vertex     */
   int32_t level_loop;         /* CGP_LOOP_*: how a traversal to convergence is driven     */
   int32_t sssp_chunk_direction; /* SSSP gather/scatter decided per 32-slot chunk from the
                                    chunk's own frontier (1), or for the whole group (-1);
@@ -122,7 +122,9 @@ typedef struct {
                                  latest admissions; 1 = whole 32-slot cohorts: requests enter
                                  only chunks whose slots are all free; 2 = group cohorts:
                                  requests enter only an empty group, all pending at once     */
-  int32_t reserved;
+  int32_t serve_groups;       /* serving loop: traversal groups the slots are split into, each
+                                 with its own masks and stream, their levels overlapping on
+                                 the device (1..8); 0 = 1                                    */
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 

@@ -37,7 +37,7 @@ class _FakeServer:
         self.capacity = capacity
         self.submits = []
 
-    def submit(self, desc):
+    def submit(self, desc, out=None):
         self.submits.append(self._clock() * 1e3)
         return len(self.submits) - 1
 

@@ -534,21 +534,39 @@ def test_sssp_gather_mixed_group(rmat_u32):
             np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
 
 
-@pytest.mark.parametrize("nq", [64, 128, 256])
+@pytest.mark.parametrize("nq", [64, 128, 256, 300, 700, 1024])
 @pytest.mark.parametrize("heavy", [0, 16, 1 << 20])
 def test_sssp_gather_light_chunks(rmat_u32, nq, heavy):
     """Light vertices gathered in CTA chunks (up to 32 vertices / 2048 in-edges,
     a larger vertex alone; with heavy_degree 2^20 every vertex is light) give
-    the same distances as one warp per vertex and as the oracle."""
+    the same distances as one warp per vertex and as the oracle; groups wider
+    than 256 slots (8 or 16 mask words, the last slice partly or wholly
+    empty) are gathered in 256-slot slices."""
     g, graph = rmat_u32
     src = g.pick_sources(nq, seed=131)
     ref, _ = oracle.batch("sssp", g, src)
     descs = [cgp.QueryDescriptor(int(s), "sssp") for s in src]
     for chunks in (True, False):
         r = cgp.run_batch(graph, descs, cgp.RunOptions(traversal_mode="pull", heavy_degree=heavy,
-                                                       light_chunks=chunks, mask_words=nq // 64),
+                                                       light_chunks=chunks,
+                                                       mask_words=nq // 64 if nq <= 256 else 0),
                           layout="query")
         np.testing.assert_array_equal(r.values, ref)
+
+
+@pytest.mark.parametrize("ratio", [0.0, 0.05, 0.5])
+def test_sssp_sliced_gather_grid_f32(grid_f32, ratio):
+    """1024 f32 SSSP queries on a grid (16 mask words): the sliced chunked
+    gather on whole-row and screened levels, mixed with scatter levels, gives
+    the oracle's distances."""
+    g, graph = grid_f32
+    src = np.resize(g.pick_sources(512, seed=141), 1024)
+    ref, _ = oracle.batch("sssp", g, src[:512])
+    r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                      cgp.RunOptions(sssp_pull_edge_ratio=ratio), layout="query")
+    v = r.values.view(np.float32)
+    np.testing.assert_array_equal(v[:512], ref)
+    np.testing.assert_array_equal(v[512:], ref)
 
 
 

@@ -141,20 +141,53 @@ def test_server_slots_bounded_by_memory(rmat):
         assert s.wait(t, 60000).state == "done"
 
 
-@pytest.mark.parametrize("policy", ["chunks", "group"])
-def test_cohort_admission_matches_oracle(rmat, policy):
+@pytest.mark.parametrize("policy,groups", [("chunks", 0), ("group", 0), ("group", 1),
+                                           ("slots", 3), ("group", 4)])
+def test_cohort_admission_matches_oracle(rmat, policy, groups):
     """Admission in whole 32-slot cohorts (requests enter only wholly free
-    chunks) or group cohorts (only an empty group takes requests) gives every
-    request its exact result."""
+    chunks) or group cohorts (only an empty group takes requests), over one
+    or several traversal groups (uneven splits included), gives every request
+    its exact result."""
     g, graph = rmat
     src = g.pick_sources(80, seed=61)
     kinds = ["bfs", "sssp", "khop"]
     descs = [cgp.QueryDescriptor(int(s), kinds[i % 3], 2 + i % 4 if i % 3 == 2 else 0)
              for i, s in enumerate(src)]
     outs = [np.zeros(g.num_vertices, np.uint32) for _ in descs]
-    with cgp.Server(graph, slots=64, options=cgp.RunOptions(serve_admission=policy)) as s:
+    opts = cgp.RunOptions(serve_admission=policy, serve_groups=groups)
+    with cgp.Server(graph, slots=64, options=opts) as s:
         tickets = [s.submit(d, o) for d, o in zip(descs, outs)]
         s.drain(timeout_ms=120000)
         assert all(s.poll(t).state == "done" for t in tickets)
+        assert s.stats()["slots"] == 64
+    for d, o in zip(descs, outs):
+        np.testing.assert_array_equal(o, _expected(g, d))
+
+
+def test_group_cohorts_overlap_staggered_arrivals():
+    """Two groups under group cohorts: requests that arrive while a cohort
+    runs in one group open a cohort in the other group, admitted before the
+    first cohort finishes, and every request still gets its exact result.
+    A 256 x 256 grid keeps the first (single-request) cohort running for
+    hundreds of levels."""
+    g = cgp.gen_grid(256, 256, 0.05, 0.0, seed=71).with_weights("u32", 1, 16, seed=72)
+    graph = cgp.CsrGraph(g)
+    src = g.pick_sources(25, seed=73)
+    descs = [cgp.QueryDescriptor(int(s), "sssp" if i % 2 == 0 else "bfs")
+             for i, s in enumerate(src)]
+    outs = [np.zeros(g.num_vertices, np.uint32) for _ in descs]
+    opts = cgp.RunOptions(serve_admission="group", serve_groups=2, levels_per_sync=1)
+    with cgp.Server(graph, slots=64, options=opts) as s:
+        first = s.submit(descs[0], outs[0])
+        deadline = time.time() + 60
+        while s.poll(first).state == "queued" and time.time() < deadline:
+            time.sleep(0.0005)
+        second = [s.submit(d, o) for d, o in zip(descs[1:], outs[1:])]
+        s.drain(timeout_ms=120000)
+        info1 = s.poll(first)
+        infos2 = [s.poll(t) for t in second]
+    assert all(i.state == "done" for i in [info1] + infos2)
+    assert info1.slot < 32 and all(i.slot >= 32 for i in infos2)
+    assert min(i.admit_ms for i in infos2) < info1.finish_ms
     for d, o in zip(descs, outs):
         np.testing.assert_array_equal(o, _expected(g, d))
