@@ -102,6 +102,7 @@ def parse_args():
     p.add_argument("--pull-frontier-ratio", type=float, default=0.15)
     p.add_argument("--heavy-degree", type=int, default=0)
     p.add_argument("--sssp-pull-edge-ratio", type=float, default=0.5)
+    p.add_argument("--sssp-pull-pair-ratio", type=float, default=0.2)
     p.add_argument("--levels-per-sync", type=int, default=0)
     p.add_argument("--level-loop", default="", choices=["", "auto", "chunks", "device"],
                    help="level loop form (default: device-looped graph for c3, else chunks)")
@@ -592,6 +593,7 @@ def run_serve(args):
                                            pull_edge_ratio=args.pull_edge_ratio,
                                            heavy_degree=args.heavy_degree,
                                            sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
+                                           sssp_pull_pair_ratio=args.sssp_pull_pair_ratio,
                                            sssp_chunk_direction=args.sssp_chunk_direction,
                                            serve_admission=args.serve_admission,
                                            serve_groups=args.serve_groups,
@@ -710,6 +712,7 @@ def main():
     tuning = dict(traversal_mode=args.mode, pull_edge_ratio=args.pull_edge_ratio,
                   pull_frontier_ratio=args.pull_frontier_ratio, heavy_degree=args.heavy_degree,
                   sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
+                  sssp_pull_pair_ratio=args.sssp_pull_pair_ratio,
                   light_chunks=not args.no_light_chunks, levels_per_sync=args.levels_per_sync,
                   level_loop=args.level_loop or ("device" if args.workload == "c3" else "chunks"))
     base = cgp.RunOptions(stream=stream.cuda_stream, **tuning)
@@ -966,6 +969,7 @@ def main():
                                     "heavy_degree": o.heavy_degree,
                                     "pull_edge_ratio": o.pull_edge_ratio,
                                     "sssp_pull_edge_ratio": o.sssp_pull_edge_ratio,
+                                    "sssp_pull_pair_ratio": o.sssp_pull_pair_ratio,
                                     "dense_unroll": o.dense_unroll, "depth_mode": o.depth_mode}
                                    for (k, _), o in zip(groups, opts)],
                        "autotuned": not args.no_autotune and args.workload in ("c1", "c2"),

@@ -41,7 +41,8 @@ class CgpOptions(Structure):
         ("discard_results", c_int32), ("profile_kernels", c_int32), ("dense_unroll", c_int32),
         ("sssp_pull_edge_ratio", c_double), ("light_chunks", c_int32), ("level_loop", c_int32),
         ("sssp_chunk_direction", c_int32), ("bfs_pull_form", c_int32),
-        ("serve_admission", c_int32), ("serve_groups", c_int32), ("stream", c_void_p),
+        ("serve_admission", c_int32), ("serve_groups", c_int32),
+        ("sssp_pull_pair_ratio", c_double), ("stream", c_void_p),
     ]
 
 

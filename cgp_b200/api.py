@@ -295,6 +295,7 @@ class RunOptions:
     profile_kernels: bool = False
     dense_unroll: int = 0
     sssp_pull_edge_ratio: float = 0.5
+    sssp_pull_pair_ratio: float = 0.2  # gather also needs est. pairs >= ratio * E * SSSP chunks
     light_chunks: bool = True
     level_loop: str = "auto"    # "auto", "chunks" (host-checked graph chunks), "device"
     sssp_chunk_direction: int = 0  # 1 per 32-slot chunk, -1 whole group, 0 auto (serving: chunk)
@@ -324,6 +325,7 @@ class RunOptions:
         o.profile_kernels = int(self.profile_kernels)
         o.dense_unroll = self.dense_unroll
         o.sssp_pull_edge_ratio = self.sssp_pull_edge_ratio
+        o.sssp_pull_pair_ratio = self.sssp_pull_pair_ratio
         o.light_chunks = 0 if self.light_chunks else -1
         if self.level_loop not in ("auto", "chunks", "device"):
             raise ValueError("level_loop must be auto, chunks or device")

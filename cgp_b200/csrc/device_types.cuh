@@ -99,6 +99,7 @@ struct LevelCtl {
   unsigned long long pull_vertex_threshold;
   unsigned long long pull_edge_threshold;
   unsigned long long sssp_pull_edge_threshold;  // gather when frontier edges reach it
+  unsigned long long sssp_pull_pair_unit;  // ... and est. pairs reach it x SSSP chunks (0: off)
   unsigned long long dense_count;  // SSSP vertices queued for the dense kernel this level
   unsigned long long hq_packed;    // heavy frontier queue: count << 40 | chunks, this level
   unsigned long long prev_improved; // SSSP entries improved by the previous level

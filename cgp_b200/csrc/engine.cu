@@ -691,6 +691,10 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
   c.prev_dir = kDirPush;
   c.sssp_pull_edge_threshold = static_cast<unsigned long long>(
       std::max(1.0, o.sssp_pull_edge_ratio * static_cast<double>(g->E)));
+  c.sssp_pull_pair_unit = o.sssp_pull_pair_ratio > 0
+                              ? static_cast<unsigned long long>(
+                                    std::max(1.0, o.sssp_pull_pair_ratio * static_cast<double>(g->E)))
+                              : 0ULL;
   ck(cudaMemcpyAsync(ws->ctl.p, &c, sizeof(LevelCtl), cudaMemcpyHostToDevice, s), "upload ctl");
 
   const uint32_t sssp_inf = g->weight_kind == CGP_WEIGHT_F32 ? 0x7f800000u : 0xffffffffu;

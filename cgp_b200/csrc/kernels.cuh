@@ -2560,20 +2560,38 @@ __device__ __forceinline__ int32_t decide_dir(const LevelCtl* ctl, unsigned long
 
 // SSSP direction of the next level: gather once the frontier's edges reach
 // the threshold (dense levels), scatter otherwise.
-__device__ __forceinline__ int32_t decide_sdir(const LevelCtl* ctl, unsigned long long edges,
-                                               bool has_sssp) {
-  if (!has_sssp || !ctl->sssp_gather) return kDirPush;
-  if (ctl->forced_dir >= 0) return ctl->forced_dir;
-  if (ctl->mode == 0) return kDirPush;
-  if (ctl->mode == 1) return kDirPull;
-  return edges >= ctl->sssp_pull_edge_threshold ? kDirPull : kDirPush;
-}
-
 template <int W>
 __device__ __forceinline__ bool any_bits(const uint64_t* m) {
   uint64_t a = 0;
   for (int i = 0; i < W; ++i) a |= m[i];
   return a != 0;
+}
+
+// Group-wide SSSP direction of a level whose frontier has `count` vertices
+// and `edges` out-edges.  Hybrid: gather when the edges reach the edge
+// threshold and the estimated (edge, slot) pairs a scatter would relax — the
+// previous level's improvements x the frontier's mean out-degree — reach
+// sssp_pull_pair_unit per SSSP 32-slot chunk: a scatter costs per pair, a
+// gather per (in-edge, gathering chunk), so a wide group whose frontier
+// carries one or two bits per vertex (a grid's first and last levels) keeps
+// scattering although its frontier touches half the edges.
+template <int W>
+__device__ __forceinline__ int32_t decide_sdir(const LevelCtl* ctl, unsigned long long count,
+                                               unsigned long long edges) {
+  if (!any_bits<W>(ctl->sssp_bits) || !ctl->sssp_gather) return kDirPush;
+  if (ctl->forced_dir >= 0) return ctl->forced_dir;
+  if (ctl->mode == 0) return kDirPush;
+  if (ctl->mode == 1) return kDirPull;
+  if (edges < ctl->sssp_pull_edge_threshold) return kDirPush;
+  if (ctl->sssp_pull_pair_unit > 0) {
+    int chunks = 0;
+    for (int i = 0; i < W; ++i)
+      chunks += (static_cast<uint32_t>(ctl->sssp_bits[i]) != 0u) + ((ctl->sssp_bits[i] >> 32) != 0ULL);
+    const double pairs = static_cast<double>(ctl->prev_improved) * static_cast<double>(edges) /
+                         static_cast<double>(count > 0 ? count : 1ULL);
+    if (pairs < static_cast<double>(ctl->sssp_pull_pair_unit) * chunks) return kDirPush;
+  }
+  return kDirPull;
 }
 
 // Splits the SSSP slots of the next level into gathering (gsel) and
@@ -2678,7 +2696,7 @@ __device__ void level_end(GroupDev& g) {
   for (int i = 0; i < W; ++i) ctl->active[par][i] = 0;
   compute_expand<W>(ctl, g.slots, g.Qg, l + 1);
   ctl->dir = decide_dir(ctl, nextc, ctl->edges[par ^ 1], any_bits<W>(ctl->bfs_bits));
-  split_sssp_slots<W>(ctl, decide_sdir(ctl, ctl->edges[par ^ 1], any_bits<W>(ctl->sssp_bits)));
+  split_sssp_slots<W>(ctl, decide_sdir<W>(ctl, nextc, ctl->edges[par ^ 1]));
   if (nextc == 0 || (ctl->max_iterations > 0 && l + 1 >= ctl->max_iterations)) {
     ctl->done = 1;
     return;
@@ -2790,7 +2808,7 @@ __global__ void k_seed(GroupDev g, DevGraph G) {
     compute_expand<W>(ctl, g.slots, g.Qg, 0);
     ctl->dir = decide_dir(ctl, ctl->count[0], ctl->edges[0], any_bits<W>(ctl->bfs_bits));
     // the sources' level: every slot starts with the group's direction
-    split_sssp_slots<W>(ctl, decide_sdir(ctl, ctl->edges[0], any_bits<W>(ctl->sssp_bits)));
+    split_sssp_slots<W>(ctl, decide_sdir<W>(ctl, ctl->count[0], ctl->edges[0]));
     if (ctl->count[0] == 0) ctl->done = 1;
   }
 }

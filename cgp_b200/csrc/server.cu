@@ -112,7 +112,7 @@ __global__ void k_admit(GroupDev g, DevGraph G, const AdmitReq* reqs, int n) {
       ctl->sdir = any_bits<W>(ctl->gsel) ? kDirPull : kDirPush;
       ctl->sscatter = any_bits<W>(ctl->ssel) ? 1 : 0;
     } else {
-      split_sssp_slots<W>(ctl, decide_sdir(ctl, ctl->edges[par], any_bits<W>(ctl->sssp_bits)));
+      split_sssp_slots<W>(ctl, decide_sdir<W>(ctl, ctl->count[par], ctl->edges[par]));
     }
   }
 }

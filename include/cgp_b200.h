@@ -125,6 +125,12 @@ typedef struct {
   int32_t serve_groups;       /* serving loop: traversal groups the slots are split into, each
                                  with its own masks and stream, their levels overlapping on
                                  the device (1..8); 0 = 1                                    */
+  double sssp_pull_pair_ratio; /* a group's SSSP level also needs the next frontier's
+                                  estimated (edge, slot) pairs (last level's improvements x
+                                  the next frontier's mean out-degree) to reach ratio x E x
+                                  the group's SSSP 32-slot chunks to gather: a scatter costs
+                                  per pair, a gather per (in-edge, chunk); default 0.2;
+                                  <= 0: edges alone decide                               */
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
 

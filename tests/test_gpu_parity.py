@@ -380,10 +380,10 @@ def test_sssp_execution_knobs_do_not_change_results(rmat_u32, opts):
 # Dense SSSP levels gather over in-edges (pull CSR + reverse-edge weights).
 @pytest.mark.parametrize("opts", [
     dict(traversal_mode="pull"),
-    dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.02),
+    dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.02, sssp_pull_pair_ratio=0.0),
     dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.0),
     dict(traversal_mode="pull", heavy_degree=16),
-    dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.05, heavy_degree=32, mask_words=16),
+    dict(traversal_mode="hybrid", sssp_pull_edge_ratio=0.05, sssp_pull_pair_ratio=0.0, heavy_degree=32, mask_words=16),
 ])
 @pytest.mark.parametrize("nq", [62, 70, 72])  # vector rows (uint2 / uint4) and scalar rows
 def test_sssp_gather_parity(rmat_u32, rmat_f32, grid_f32, opts, nq):
@@ -423,7 +423,7 @@ def test_sssp_gather_uses_reverse_edge_weights(kind):
     ref, _ = oracle.batch("sssp", g, src)
     for mode in ("push", "pull", "hybrid"):
         r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
-                          cgp.RunOptions(traversal_mode=mode, sssp_pull_edge_ratio=0.01),
+                          cgp.RunOptions(traversal_mode=mode, sssp_pull_edge_ratio=0.01, sssp_pull_pair_ratio=0.0),
                           layout="query")
         np.testing.assert_array_equal(r.values, ref)
 
@@ -451,7 +451,7 @@ def test_sssp_gather_unsorted_lists_and_directed():
         ref, _ = oracle.batch("sssp", g, src)
         for mode in ("pull", "hybrid"):
             r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
-                              cgp.RunOptions(traversal_mode=mode, sssp_pull_edge_ratio=0.01,
+                              cgp.RunOptions(traversal_mode=mode, sssp_pull_edge_ratio=0.01, sssp_pull_pair_ratio=0.0,
                                              heavy_degree=24), layout="query")
             np.testing.assert_array_equal(r.values, ref)
 
@@ -463,7 +463,7 @@ def test_mixed_batch_with_sssp_gather(rmat_u32, ratio):
     kinds = ["bfs", "sssp", "khop", "sssp"]
     descs = [cgp.QueryDescriptor(int(s), kinds[i % 4], 2) for i, s in enumerate(src)]
     r = cgp.run_heterogeneous(graph, cgp.HybridQueryBatch(descs),
-                              options=cgp.RunOptions(sssp_pull_edge_ratio=ratio), layout="query")
+                              options=cgp.RunOptions(sssp_pull_edge_ratio=ratio, sssp_pull_pair_ratio=0.0), layout="query")
     for i, d in enumerate(descs):
         if d.kind == "bfs":
             np.testing.assert_array_equal(r.values[i].view(np.int32), oracle.bfs(g, d.source))
@@ -502,7 +502,7 @@ def test_large_mixed_batch_split_by_kind(rmat_u32, layout, order):
 
 @pytest.mark.parametrize("wrange", [(1, 64), (500, 4000), (1 << 20, 1 << 21), (1 << 30, 3 << 30)])
 @pytest.mark.parametrize("opts", [dict(traversal_mode="pull"),
-                                  dict(sssp_pull_edge_ratio=0.05, heavy_degree=32)])
+                                  dict(sssp_pull_edge_ratio=0.05, sssp_pull_pair_ratio=0.0, heavy_degree=32)])
 def test_sssp_gather_weight_ranges(wrange, opts):
     """256-slot gathers and scatters with small, medium, large and near-overflow
     integer weights (sums saturate at UINT32_MAX exactly like the oracle's)."""
@@ -534,6 +534,27 @@ def test_sssp_gather_mixed_group(rmat_u32):
             np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
 
 
+def test_sssp_pair_condition_keeps_sparse_levels_scattering(grid_f32):
+    """A 1024-slot group on a grid: with the pair condition a level gathers
+    only when its estimated (edge, slot) pairs are worth a gather, so no more
+    levels gather than with the edge condition alone; the distances are the
+    oracle's either way."""
+    g, graph = grid_f32
+    src = np.resize(g.pick_sources(512, seed=143), 1024)
+    ref, _ = oracle.batch("sssp", g, src[:512])
+    gathers = {}
+    for pr in (0.0, 0.2):
+        r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
+                          cgp.RunOptions(sssp_pull_edge_ratio=0.05, sssp_pull_pair_ratio=pr,
+                                         profile_iterations=True), layout="query")
+        v = r.values.view(np.float32)
+        np.testing.assert_array_equal(v[:512], ref)
+        np.testing.assert_array_equal(v[512:], ref)
+        gathers[pr] = sum(p.sssp_mode == "pull" for p in r.iteration_profiles)
+    assert gathers[0.0] > 0
+    assert gathers[0.2] <= gathers[0.0]
+
+
 @pytest.mark.parametrize("nq", [64, 128, 256, 300, 700, 1024])
 @pytest.mark.parametrize("heavy", [0, 16, 1 << 20])
 def test_sssp_gather_light_chunks(rmat_u32, nq, heavy):
@@ -563,7 +584,7 @@ def test_sssp_sliced_gather_grid_f32(grid_f32, ratio):
     src = np.resize(g.pick_sources(512, seed=141), 1024)
     ref, _ = oracle.batch("sssp", g, src[:512])
     r = cgp.run_batch(graph, [cgp.QueryDescriptor(int(s), "sssp") for s in src],
-                      cgp.RunOptions(sssp_pull_edge_ratio=ratio), layout="query")
+                      cgp.RunOptions(sssp_pull_edge_ratio=ratio, sssp_pull_pair_ratio=0.0), layout="query")
     v = r.values.view(np.float32)
     np.testing.assert_array_equal(v[:512], ref)
     np.testing.assert_array_equal(v[512:], ref)
@@ -659,7 +680,7 @@ def test_sssp_direction_per_chunk(rmat_paths, nq, kinds, ratio):
                  for i, s in enumerate(src)]
     else:
         descs = [cgp.QueryDescriptor(int(s), "sssp") for s in src]
-    opts = cgp.RunOptions(sssp_chunk_direction=1, sssp_pull_edge_ratio=ratio, mask_words=16)
+    opts = cgp.RunOptions(sssp_chunk_direction=1, sssp_pull_edge_ratio=ratio, sssp_pull_pair_ratio=0.0, mask_words=16)
     r = cgp.run_batch(graph, descs, opts, layout="query")
     for i, d in enumerate(descs):
         exp = oracle.bfs(g, d.source).view(np.uint32) if d.kind == "bfs" else oracle.sssp(g, d.source)
@@ -672,7 +693,7 @@ def test_sssp_direction_per_chunk_f32_grid(grid_paths):
     descs = [cgp.QueryDescriptor(int(s), "sssp") for s in src]
     for loop in ("chunks", "device"):
         r = cgp.run_batch(graph, descs, cgp.RunOptions(sssp_chunk_direction=1,
-                                                       sssp_pull_edge_ratio=0.05,
+                                                       sssp_pull_edge_ratio=0.05, sssp_pull_pair_ratio=0.0,
                                                        level_loop=loop), layout="query")
         ref, _ = oracle.batch("sssp", g, src)
         np.testing.assert_array_equal(r.values.view(np.float32), ref)
