@@ -103,6 +103,9 @@ def parse_args():
     p.add_argument("--heavy-degree", type=int, default=0)
     p.add_argument("--sssp-pull-edge-ratio", type=float, default=0.5)
     p.add_argument("--sssp-pull-pair-ratio", type=float, default=0.2)
+    p.add_argument("--bfs-pull-form", type=int, default=0, choices=[0, 1, 2],
+                   help="BFS pull: lane per vertex (0), CTA chunks (1), lane per vertex in "
+                        "in-degree order (2)")
     p.add_argument("--levels-per-sync", type=int, default=0)
     p.add_argument("--level-loop", default="", choices=["", "auto", "chunks", "device"],
                    help="level loop form (default: device-looped graph for c3, else chunks)")
@@ -713,6 +716,7 @@ def main():
                   pull_frontier_ratio=args.pull_frontier_ratio, heavy_degree=args.heavy_degree,
                   sssp_pull_edge_ratio=args.sssp_pull_edge_ratio,
                   sssp_pull_pair_ratio=args.sssp_pull_pair_ratio,
+                  bfs_pull_form=args.bfs_pull_form,
                   light_chunks=not args.no_light_chunks, levels_per_sync=args.levels_per_sync,
                   level_loop=args.level_loop or ("device" if args.workload == "c3" else "chunks"))
     base = cgp.RunOptions(stream=stream.cuda_stream, **tuning)

@@ -300,6 +300,8 @@ class RunOptions:
     level_loop: str = "auto"    # "auto", "chunks" (host-checked graph chunks), "device"
     sssp_chunk_direction: int = 0  # 1 per 32-slot chunk, -1 whole group, 0 auto (serving: chunk)
     bfs_pull_chunks: bool = False  # CTA-chunked light-vertex BFS pull on levels that read most edges
+    bfs_pull_form: int = 0  # 0 lane per vertex (vertex order), 1 CTA chunks, 2 lane per vertex
+                            # in decreasing in-degree order (bfs_pull_chunks=True means 1)
     serve_admission: str = "slots"  # serving: "slots" (any free slot), "chunks" (whole 32-slot
                                     # cohorts) or "group" (a new cohort only in an empty group)
     serve_groups: int = 0  # serving: traversal groups, each on its own stream (0 = 1)
@@ -332,7 +334,9 @@ class RunOptions:
         o.level_loop = {"auto": N.LOOP_AUTO, "chunks": N.LOOP_CHUNKS,
                         "device": N.LOOP_DEVICE}[self.level_loop]
         o.sssp_chunk_direction = int(self.sssp_chunk_direction)
-        o.bfs_pull_form = 1 if self.bfs_pull_chunks else 0
+        if self.bfs_pull_form not in (0, 1, 2):
+            raise ValueError("bfs_pull_form must be 0, 1 or 2")
+        o.bfs_pull_form = 1 if self.bfs_pull_chunks else int(self.bfs_pull_form)
         if self.serve_admission not in ("slots", "chunks", "group"):
             raise ValueError("serve_admission must be slots, chunks or group")
         o.serve_admission = {"slots": 0, "chunks": 1, "group": 2}[self.serve_admission]

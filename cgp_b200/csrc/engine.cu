@@ -687,7 +687,8 @@ void group_prepare(GraphImpl* g, Workspace* ws, GroupSpec& spec, const cgp_optio
       std::max(1.0, o.pull_edge_ratio * static_cast<double>(g->E)));
   c.sssp_gather = sssp_gather_on(g, o) ? 1 : 0;
   c.chunk_dir = sssp_chunk_dir(spec, o) ? 1 : 0;
-  c.bfs_chunked = (spec.has_bfs && o.bfs_pull_form > 0 && hp.plight.chunks > 0) ? 1 : 0;
+  c.bfs_chunked = (spec.has_bfs && (o.bfs_pull_form == 1 || o.bfs_pull_form == 2) &&
+                   hp.plight.chunks > 0) ? o.bfs_pull_form : 0;
   c.prev_dir = kDirPush;
   c.sssp_pull_edge_threshold = static_cast<unsigned long long>(
       std::max(1.0, o.sssp_pull_edge_ratio * static_cast<double>(g->E)));
@@ -731,7 +732,7 @@ int enqueue_levels(GraphImpl* g, Workspace* ws, const GroupSpec& spec, const cgp
   if (!g->can_gather()) mode = CGP_MODE_PUSH;
   L.pull = mode != CGP_MODE_PUSH;
   L.heavy_push = L.G.n_heavy > 0 || g->max_degree > 32;
-  L.bfs_chunked = L.pull && spec.has_bfs && L.G.n_plight_chunks > 0 && o.bfs_pull_form > 0;
+  L.bfs_chunked = L.pull && spec.has_bfs && L.G.n_plight_chunks > 0 && o.bfs_pull_form == 1;
   L.spull = spec.has_sssp && sssp_gather_on(g, o);
   {
     // vector gather: kElem-slot vectors must stay inside rows and be aligned

@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(kBlock) k_bfs_push_heavy(GroupDev g, DevGraph 
 // levels (bits are still rare, almost every in-edge is read) and levels after
 // a pull level that read at least half of the in-edges.
 __device__ __forceinline__ bool bfs_pull_chunked_level(const LevelCtl* ctl, int64_t E) {
-  if (!ctl->bfs_chunked) return false;
+  if (ctl->bfs_chunked != 1) return false;
   return ctl->prev_dir != kDirPull || 2 * ctl->prev_pull_edges >= static_cast<unsigned long long>(E);
 }
 
@@ -574,9 +574,10 @@ template <int W>
 __global__ void __launch_bounds__(kBlock) k_clear_next(GroupDev g, int64_t E) {
   const LevelCtl* ctl = g.ctl;
   if (ctl->done) return;
-  // a lane-per-vertex pull level rewrites every vertex's next mask; the
-  // chunked one writes only vertices with new bits
-  if (ctl->dir != kDirPush && !bfs_pull_chunked_level(ctl, E)) return;
+  // a lane-per-vertex pull level in vertex order rewrites every vertex's next
+  // mask; the chunked one and the in-degree-ordered one (which skips vertices
+  // without in-edges) write only the vertices they pull
+  if (ctl->dir != kDirPush && !bfs_pull_chunked_level(ctl, E) && ctl->bfs_chunked != 2) return;
   const LevelView lv = level_view(g);
   const unsigned long long n = ctl->prev_count;
   const int32_t* plist = lv.nlist;  // list of the previous frontier
@@ -625,7 +626,11 @@ __device__ __forceinline__ bool bfs_pull_uses_summary(const GroupDev& g, const L
 // Pull level (bottom-up): every non-heavy vertex with unvisited active bits
 // ORs the current-frontier masks of its in-neighbours until every needed bit
 // is found (early exit).  Reads only the current frontier, so depths are
-// exactly level-synchronous.
+// exactly level-synchronous.  Vertex order by default (a tile is 32
+// consecutive vertices); with bfs_chunked == 2 the tiles run over the light
+// table's vertices of in-degree 1..32 in decreasing in-degree order, so the
+// lanes of a warp walk lists of about the same length (the next masks of the
+// vertices left out are zeroed by k_clear_next).
 template <int W, typename OT, int DEPTH>
 __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev g, DevGraph G) {
   const LevelCtl* ctl = g.ctl;
@@ -645,11 +650,15 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
 #pragma unroll
   for (int i = 0; i < W; ++i) uni[i] = 0;
   unsigned long long pairs = 0, pverts = 0, pedges = 0;
+  const bool sorted = ctl->bfs_chunked == 2;
+  // tiles over vertex ids, or over the light table's entries n_pmid .. end
+  const unsigned long long n_items =
+      sorted ? static_cast<unsigned long long>(G.plight_chunk_start[G.n_plight_chunks] - G.n_pmid) : V;
 
-  for (unsigned long long tile = gw; tile * 32 < V; tile += nwarps) {
+  for (unsigned long long tile = gw; tile * 32 < n_items; tile += nwarps) {
     const unsigned long long vv = tile * 32 + lane;
-    const bool valid = vv < V;
-    const int32_t v = static_cast<int32_t>(valid ? vv : 0);
+    const bool valid = vv < n_items;
+    const int32_t v = !valid ? 0 : sorted ? G.plight[G.n_pmid + vv] : static_cast<int32_t>(vv);
     uint64_t vis[W], need[W], acc[W];
     int64_t beg = 0, end = 0;
 #pragma unroll
@@ -2199,6 +2208,20 @@ __global__ void __launch_bounds__(kBlock, (W == 4 ? 4 : (W <= 8 ? 3 : 2))) k_sss
   warp_add(verts, &g.ctl->lc.spull_vertices, lane);
 }
 
+// Owner of in-edge f0 + lane in a chunk whose vertex k starts at prefix
+// position pre_k (lane k passes its own pre_k, INT_MAX beyond the chunk;
+// every chunk vertex has an in-edge, so the starts are distinct): the last k
+// with pre_k <= f0 + lane.  One ballot and one OR-reduction per 32 in-edges
+// instead of a binary search per lane.  All lanes call.
+__device__ __forceinline__ int chunk_edge_owner(int my_pre, int f0, int lane) {
+  const int k0 = __popc(__ballot_sync(kFull, my_pre <= f0)) - 1;
+  // bit (pre_k - f0) for the vertices that start inside (f0, f0 + 32)
+  const unsigned d = static_cast<unsigned>(my_pre - f0 - 1);
+  const unsigned starts = __reduce_or_sync(kFull, d < 31u ? 2u << d : 0u);
+  const unsigned upto = lane == 31 ? 0xffffffffu : (2u << lane) - 1u;
+  return k0 + __popc(starts & upto);
+}
+
 // Gather level (vectorised), light vertices in CTA chunks.  A chunk is a
 // run of up to kLightChunkVerts light vertices with at most kLightChunkEdges
 // in-edges in total (static table of the pull CSR).  The CTA's warps split
@@ -2298,18 +2321,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
     int4* stage = s_stage[wib];
     for (int f0 = fa; f0 < fb; f0 += 32) {
       const int f = f0 + lane;
-      int cnt = 0, k = 0;
+      int cnt = 0;
       int32_t u = 0;
       uint32_t wb = 0;
       uint32_t cm = 0xffffffffu;  // 32-slot chunks of the source row to read
+      const int k = chunk_edge_owner(lane < nv ? s_pre[lane] : 0x7fffffff, f0, lane);
       if (f < fb) {
-        int lo = 0, hi = nv - 1;  // owner: last k with s_pre[k] <= f
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (s_pre[mid] <= f) lo = mid;
-          else hi = mid - 1;
-        }
-        k = lo;
         const int64_t e = s_beg[k] + (f - s_pre[k]);
         u = G.pcol[e];
         wb = weight_bits<WK>(G.pw, e);

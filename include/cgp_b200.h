@@ -115,9 +115,10 @@ typedef struct {
                                    chunk's own frontier (1), or for the whole group (-1);
                                    0 = auto: per chunk in the serving loop, whole group in
                                    batch runs                                              */
-  int32_t bfs_pull_form;      /* light-vertex BFS pull: 0 = a lane per vertex on every pull
-                                 level; 1 = CTA chunks on pull levels that read most in-edges
-                                 (measured slower on R-MAT: kept as an option)               */
+  int32_t bfs_pull_form;      /* light-vertex BFS pull: 0 = a lane per vertex, vertex order;
+                                 1 = CTA chunks on pull levels that read most in-edges
+                                 (measured slower on R-MAT: kept as an option); 2 = a lane
+                                 per vertex, vertices in decreasing in-degree order          */
   int32_t serve_admission;    /* serving loop: 0 = any free slot, preferring the chunk of the
                                  latest admissions; 1 = whole 32-slot cohorts: requests enter
                                  only chunks whose slots are all free; 2 = group cohorts:

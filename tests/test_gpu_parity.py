@@ -701,12 +701,44 @@ def test_sssp_direction_per_chunk_f32_grid(grid_paths):
 
 @pytest.mark.parametrize("nq", [1, 64, 200, 256])
 @pytest.mark.parametrize("depth", ["planes", "direct"])
-def test_bfs_chunked_pull_option(rmat_u32, nq, depth):
-    """The CTA-chunked light-vertex pull (opt-in) gives the oracle's depths."""
+@pytest.mark.parametrize("form", [1, 2])
+def test_bfs_pull_form_options(rmat_u32, nq, depth, form):
+    """The CTA-chunked light-vertex pull (form 1) and the lane pull in
+    in-degree order (form 2, next masks of vertices without in-edges zeroed
+    by k_clear_next) give the oracle's depths, with and without the
+    in-degree 33..heavy kernel (heavy_degree 64 / 16)."""
     g, graph = rmat_u32
     src = g.pick_sources(nq, seed=90 + nq)
     ref, _ = oracle.batch("bfs", g, src)
-    for ratio in (0.01, 0.2):
-        r = _bfs(src, graph, cgp.RunOptions(bfs_pull_chunks=True, pull_edge_ratio=ratio,
-                                            depth_mode=depth, heavy_degree=64))
+    for ratio, heavy in ((0.01, 64), (0.2, 64), (0.05, 16)):
+        r = _bfs(src, graph, cgp.RunOptions(bfs_pull_form=form, pull_edge_ratio=ratio,
+                                            depth_mode=depth, heavy_degree=heavy))
         np.testing.assert_array_equal(r.values, ref)
+
+
+def test_bfs_pull_in_degree_order_mixed_and_directed(rmat_u32):
+    """Form 2 on a mixed BFS / k-hop / SSSP group and on a directed graph
+    (pull over the transpose)."""
+    g, graph = rmat_u32
+    src = g.pick_sources(96, seed=97)
+    descs = [cgp.QueryDescriptor(int(s), ["bfs", "khop", "sssp"][i % 3], 3)
+             for i, s in enumerate(src)]
+    r = cgp.run_heterogeneous(graph, cgp.HybridQueryBatch(descs),
+                              options=cgp.RunOptions(bfs_pull_form=2, pull_edge_ratio=0.02),
+                              layout="query")
+    for i, d in enumerate(descs):
+        if d.kind == "sssp":
+            np.testing.assert_array_equal(r.values[i], oracle.sssp(g, d.source))
+        else:
+            exp = oracle.bfs(g, d.source, 3) if d.kind == "khop" else oracle.bfs(g, d.source)
+            np.testing.assert_array_equal(r.values[i].view(np.int32), exp)
+    rng = np.random.default_rng(98)
+    V = 3000
+    a = rng.integers(0, V, 24000)
+    b = rng.integers(0, V, 24000)
+    dg = cgp.csr_from_edges(V, a, b, symmetrize=False)
+    dgraph = cgp.CsrGraph(dg)
+    ds = dg.pick_sources(64, seed=99)
+    ref, _ = oracle.batch("bfs", dg, ds)
+    r = _bfs(ds, dgraph, cgp.RunOptions(bfs_pull_form=2, traversal_mode="pull"))
+    np.testing.assert_array_equal(r.values, ref)
