@@ -102,7 +102,7 @@ def parse_args():
     p.add_argument("--pull-frontier-ratio", type=float, default=0.15)
     p.add_argument("--heavy-degree", type=int, default=0)
     p.add_argument("--sssp-pull-edge-ratio", type=float, default=0.5)
-    p.add_argument("--sssp-pull-pair-ratio", type=float, default=0.2)
+    p.add_argument("--sssp-pull-pair-ratio", type=float, default=0.5)
     p.add_argument("--bfs-pull-form", type=int, default=0, choices=[0, 1, 2],
                    help="BFS pull: lane per vertex (0), CTA chunks (1), lane per vertex in "
                         "in-degree order (2)")

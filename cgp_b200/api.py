@@ -295,7 +295,7 @@ class RunOptions:
     profile_kernels: bool = False
     dense_unroll: int = 0
     sssp_pull_edge_ratio: float = 0.5
-    sssp_pull_pair_ratio: float = 0.2  # gather also needs est. pairs >= ratio * E * SSSP chunks
+    sssp_pull_pair_ratio: float = 0.5  # gather also needs est. pairs >= ratio * E * SSSP chunks
     light_chunks: bool = True
     level_loop: str = "auto"    # "auto", "chunks" (host-checked graph chunks), "device"
     sssp_chunk_direction: int = 0  # 1 per 32-slot chunk, -1 whole group, 0 auto (serving: chunk)

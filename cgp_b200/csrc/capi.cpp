@@ -53,7 +53,7 @@ cgp_status cgp_options_init(cgp_options* o) {
   o->pull_frontier_ratio = 0.15;
   o->pull_edge_ratio = 0.20;
   o->sssp_pull_edge_ratio = 0.5;
-  o->sssp_pull_pair_ratio = 0.2;
+  o->sssp_pull_pair_ratio = 0.5;
   o->use_cuda_graph = 1;
   o->depth_mode = CGP_DEPTH_AUTO;
   return CGP_OK;

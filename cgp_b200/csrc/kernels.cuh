@@ -659,17 +659,17 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
     const unsigned long long vv = tile * 32 + lane;
     const bool valid = vv < n_items;
     const int32_t v = !valid ? 0 : sorted ? G.plight[G.n_pmid + vv] : static_cast<int32_t>(vv);
-    uint64_t vis[W], need[W], acc[W];
+    uint64_t need[W], acc[W];
     int64_t beg = 0, end = 0;
 #pragma unroll
     for (int i = 0; i < W; ++i) {
-      vis[i] = 0;
       need[i] = 0;
       acc[i] = 0;
     }
     if (valid) {
       beg = row_at<OT>(G.prow, v);
       end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
+      uint64_t vis[W];
       load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
 #pragma unroll
       for (int i = 0; i < W; ++i) need[i] = ~vis[i] & act[i];
@@ -746,9 +746,12 @@ __global__ void __launch_bounds__(kBlock, (W <= 4 ? 3 : 1)) k_bfs_pull(GroupDev 
     }
     bool app = false;
     if (valid && !heavy) {
-      uint64_t nwm[W];
+      uint64_t nwm[W], vis[W];
 #pragma unroll
       for (int i = 0; i < W; ++i) nwm[i] = acc[i] & need[i];
+      // visited again (this warp's vertex: unchanged since the tile began);
+      // not kept in registers across the in-edge loop
+      load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
       pull_commit<W, DEPTH>(g, G.V, lv, v, vis, nwm, uni, pairs);
       app = mask_any<W>(nwm);
     }

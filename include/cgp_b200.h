@@ -130,7 +130,7 @@ typedef struct {
                                   estimated (edge, slot) pairs (last level's improvements x
                                   the next frontier's mean out-degree) to reach ratio x E x
                                   the group's SSSP 32-slot chunks to gather: a scatter costs
-                                  per pair, a gather per (in-edge, chunk); default 0.2;
+                                  per pair, a gather per (in-edge, chunk); default 0.5;
                                   <= 0: edges alone decide                               */
   void* stream;               /* cudaStream_t; NULL = the library's own stream   */
 } cgp_options;
