@@ -138,6 +138,8 @@ struct DevGraph {
   int64_t heavy_degree;
   const int32_t* plight;             // light vertices of the pull CSR (chunked gathers)
   const int32_t* plight_chunk_start; // [n_plight_chunks + 1]
+  const int64_t* plight_beg;         // first pull-CSR in-edge of plight[i]
+  const int32_t* plight_pre;         // in-edges of plight[i]'s chunk up to and including it
   int32_t n_plight_chunks;
   int32_t n_pmid;                    // plight[0 .. n_pmid) have in-degree > 32 (BFS pull mid kernel)
 };

@@ -152,6 +152,8 @@ DevGraph GraphImpl::dev_graph(int64_t h) {
   d.pheavy_chunks = hp.pheavy.chunks;
   d.plight = hp.plight.vertices.as<int32_t>();
   d.plight_chunk_start = hp.plight.chunk_start.as<int32_t>();
+  d.plight_beg = hp.plight.beg.as<int64_t>();
+  d.plight_pre = hp.plight.pre.as<int32_t>();
   d.n_plight_chunks = hp.plight.chunks;
   d.n_pmid = hp.plight.n_mid;
   d.heavy_degree = h;
@@ -220,11 +222,31 @@ void build_light_chunks(const std::vector<int64_t>& row, int64_t V, int64_t h, L
   t.chunks = static_cast<int32_t>(cs.size()) - 1;
   t.n_mid = 0;
   while (t.n_mid < t.n && row[vs[t.n_mid] + 1] - row[vs[t.n_mid]] > 32) ++t.n_mid;
+  // per entry: its first in-edge and the chunk's in-edges up to and including
+  // it, so that a chunk's header is three independent loads
+  std::vector<int64_t> beg(vs.size());
+  std::vector<int32_t> pre(vs.size());
+  for (size_t c = 0; c + 1 < cs.size(); ++c) {
+    int32_t acc = 0;
+    for (int32_t i = cs[c]; i < cs[c + 1]; ++i) {
+      const int32_t v = vs[i];
+      beg[i] = row[v];
+      acc += static_cast<int32_t>(row[v + 1] - row[v]);
+      pre[i] = acc;
+    }
+  }
   t.vertices.ensure(std::max<size_t>(vs.size(), 1) * sizeof(int32_t));
   t.chunk_start.ensure(cs.size() * sizeof(int32_t));
-  if (!vs.empty())
+  t.beg.ensure(std::max<size_t>(vs.size(), 1) * sizeof(int64_t));
+  t.pre.ensure(std::max<size_t>(vs.size(), 1) * sizeof(int32_t));
+  if (!vs.empty()) {
     ck(cudaMemcpy(t.vertices.p, vs.data(), vs.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
        "upload light vertices");
+    ck(cudaMemcpy(t.beg.p, beg.data(), beg.size() * sizeof(int64_t), cudaMemcpyHostToDevice),
+       "upload light offsets");
+    ck(cudaMemcpy(t.pre.p, pre.data(), pre.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+       "upload light prefixes");
+  }
   ck(cudaMemcpy(t.chunk_start.p, cs.data(), cs.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
      "upload light chunks");
 }

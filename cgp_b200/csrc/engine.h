@@ -57,6 +57,8 @@ struct HeavyTable {
 struct LightChunks {
   DevBuf vertices;     // int32 [n] light vertices, largest in-degree first
   DevBuf chunk_start;  // int32 [chunks + 1] positions in `vertices`
+  DevBuf beg;          // int64 [n] first in-edge of each vertex in the pull CSR
+  DevBuf pre;          // int32 [n] in-edges of the chunk up to and including the vertex
   int32_t n = 0;
   int32_t chunks = 0;
   int32_t n_mid = 0;   // the first n_mid have in-degree > 32

@@ -2281,24 +2281,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
     const int cs = G.plight_chunk_start[c];
     const int nv = G.plight_chunk_start[c + 1] - cs;
     if (wib == 0) {
-      int32_t v = 0;
-      int64_t b = 0;
-      int d = 0;
+      // vertex, first in-edge and in-edge prefix come from the table: three
+      // independent loads (no chain through the offsets)
       if (lane < nv) {
-        v = G.plight[cs + lane];
-        b = row_at<OT>(G.prow, v);
-        d = static_cast<int>(row_at<OT>(G.prow, static_cast<int64_t>(v) + 1) - b);
-      }
-      int inc = d;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(kFull, inc, o);
-        if (lane >= o) inc += t;
-      }
-      if (lane < nv) {
-        s_v[lane] = v;
-        s_beg[lane] = b;
-        s_pre[lane + 1] = inc;
+        s_v[lane] = G.plight[cs + lane];
+        s_beg[lane] = G.plight_beg[cs + lane];
+        s_pre[lane + 1] = G.plight_pre[cs + lane];
       }
       if (lane == 0) s_pre[0] = 0;
     }
