@@ -76,6 +76,8 @@ struct LevelCtl {
   uint64_t sssp_bits[kMaxW];    // slots with min-reduce semantics (SSSP)
   uint64_t gsel[kMaxW];         // SSSP slots that gather (pull) at the current level
   uint64_t ssel[kMaxW];         // SSSP slots that scatter (push) at the current level
+  unsigned long long cpairs[2 * kMaxW];  // per 32-slot chunk: (out-edge, SSSP bit) pairs of
+                                         // the next frontier (what a scatter would relax)
   unsigned long long cedges[2 * kMaxW];  // per 32-slot chunk: out-edges of the next
                                          // frontier's vertices with an SSSP bit in it
   unsigned long long sssp_chunk_levels;    // sum over levels of chunks with SSSP slots

@@ -2606,9 +2606,11 @@ __device__ __forceinline__ int32_t decide_sdir(const LevelCtl* ctl, unsigned lon
 // scattering (ssel) ones.  Group-wide by default (every slot takes
 // `group_dir`); with chunk_dir in hybrid mode each 32-slot chunk gathers when
 // the out-edges of the next frontier's vertices that carry one of its bits
-// (cedges, summed by k_chunk_census) reach the gather threshold, so a few
-// queries in their dense phase do not make every other slot gather too.
-// Consumes (zeroes) cedges.
+// (cedges, summed by k_chunk_census) reach the gather threshold and the
+// chunk's (edge, slot) pairs (cpairs) reach sssp_pull_pair_unit, so a few
+// queries in their dense phase do not make every other slot gather too, and a
+// chunk whose last improvements are few scatters them.  Consumes (zeroes)
+// cedges and cpairs.
 template <int W>
 __device__ __forceinline__ void split_sssp_slots(LevelCtl* ctl, int32_t group_dir) {
   const bool per_chunk = ctl->chunk_dir && ctl->mode == 2 && ctl->forced_dir < 0 &&
@@ -2619,7 +2621,11 @@ __device__ __forceinline__ void split_sssp_slots(LevelCtl* ctl, int32_t group_di
     if (per_chunk) {
       for (int h = 0; h < 2; ++h) {
         const uint64_t half = 0xffffffffULL << (32 * h);
-        if (ctl->cedges[2 * i + h] >= ctl->sssp_pull_edge_threshold) gm |= half;
+        // as the group rule: enough frontier edges, and enough (edge, slot)
+        // pairs that a scatter would cost more than the chunk's gather
+        if (ctl->cedges[2 * i + h] >= ctl->sssp_pull_edge_threshold &&
+            (ctl->sssp_pull_pair_unit == 0 || ctl->cpairs[2 * i + h] >= ctl->sssp_pull_pair_unit))
+          gm |= half;
       }
     } else if (group_dir == kDirPull) {
       gm = ~0ULL;
@@ -2633,7 +2639,7 @@ __device__ __forceinline__ void split_sssp_slots(LevelCtl* ctl, int32_t group_di
       ctl->gather_chunk_levels += static_cast<uint32_t>(ctl->gsel[i] >> (32 * h)) != 0u;
     }
   }
-  for (int c = 0; c < 2 * kMaxW; ++c) ctl->cedges[c] = 0;
+  for (int c = 0; c < 2 * kMaxW; ++c) ctl->cedges[c] = ctl->cpairs[c] = 0;
   ctl->sdir = g_any ? kDirPull : kDirPush;
   ctl->sscatter = s_any ? 1 : 0;
 }
@@ -2735,9 +2741,9 @@ __global__ void __launch_bounds__(kBlock) k_chunk_census(GroupDev g, DevGraph G)
   const LevelView lv = level_view(g);
   const unsigned long long n = *lv.ncount;
   const int lane = threadIdx.x & 31;
-  unsigned long long acc[2 * W];
+  unsigned long long acc[2 * W], pacc[2 * W];
 #pragma unroll
-  for (int c = 0; c < 2 * W; ++c) acc[c] = 0;
+  for (int c = 0; c < 2 * W; ++c) acc[c] = pacc[c] = 0;
   const unsigned long long stride = static_cast<unsigned long long>(gridDim.x) * blockDim.x;
   for (unsigned long long i0 = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
        i0 < n; i0 += stride) {
@@ -2750,17 +2756,26 @@ __global__ void __launch_bounds__(kBlock) k_chunk_census(GroupDev g, DevGraph G)
 #pragma unroll
       for (int w = 0; w < W; ++w) {
         const uint64_t x = m[w] & ctl->sssp_bits[w];
-        if (static_cast<uint32_t>(x)) acc[2 * w] += d;
-        if (static_cast<uint32_t>(x >> 32)) acc[2 * w + 1] += d;
+        const int lo = __popc(static_cast<uint32_t>(x)), hi = __popc(static_cast<uint32_t>(x >> 32));
+        if (lo) acc[2 * w] += d;
+        if (hi) acc[2 * w + 1] += d;
+        pacc[2 * w] += d * static_cast<unsigned long long>(lo);
+        pacc[2 * w + 1] += d * static_cast<unsigned long long>(hi);
       }
     }
   }
 #pragma unroll
   for (int c = 0; c < 2 * W; ++c) {
-    unsigned long long x = acc[c];
+    unsigned long long x = acc[c], y = pacc[c];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
-    if (lane == 0 && x) atomicAdd(&ctl->cedges[c], x);
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_xor_sync(kFull, x, o);
+      y += __shfl_xor_sync(kFull, y, o);
+    }
+    if (lane == 0 && x) {
+      atomicAdd(&ctl->cedges[c], x);
+      atomicAdd(&ctl->cpairs[c], y);
+    }
   }
 }
 
