@@ -275,7 +275,7 @@ struct cgp_server {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   }
   void loop();
-  int pick_slot(int* group);
+  int pick_slot(int* group, int32_t kind);
   void finish_wcc(std::vector<uint64_t>& tickets);
   void retire(ServeGroup& gr, std::vector<int>& local_slots, bool forced);
   void release_pinned();
@@ -454,13 +454,41 @@ void cgp_server::retire(ServeGroup& gr, std::vector<int>& to_retire, bool forced
 //    filling in this pass, so each group runs one cohort at a time and every
 //    gather level of the group serves all of its SSSP requests; with two or
 //    more groups, arrivals open a cohort in an idle group while the others
-//    run, and the groups' levels overlap on the device.
-// (Separating SSSP from BFS-like requests into chunks of their own was
-// measured too: lower capacity on R-MAT 24, 329 against 380 q/s at 500 q/s
+//    run, and the groups' levels overlap on the device.  Inside the group,
+//    SSSP requests fill the slots from the bottom and BFS-like ones from the
+//    top, so a gather reads only the chunks that hold SSSP slots.
+// (Separating SSSP from BFS-like requests into chunks of their own under the
+// free-slot policy was measured too: lower capacity on R-MAT 24, 329 against
+// 380 q/s at 500 q/s
 // offered, since a saturated server refills single freed slots and an
 // all-SSSP chunk then gathers at most levels.)
-int cgp_server::pick_slot(int* group) {
+int cgp_server::pick_slot(int* group, int32_t kind) {
   const int pol = o.serve_admission;
+  if (pol == 2) {
+    // group cohorts: the group this pass fills, else an empty one; inside it
+    // SSSP requests take the lowest free slots and BFS-like ones the highest,
+    // so the cohort's SSSP slots share as few 32-slot chunks as possible and
+    // its gather levels read only those chunks of each source row
+    int gsel = -1;
+    for (int gi = 0; gi < static_cast<int>(groups.size()); ++gi) {
+      const ServeGroup& gr = groups[gi];
+      if (gr.nadmit > 0 && gr.nadmit < gr.S) {
+        gsel = gi;
+        break;
+      }
+      if (gsel < 0 && !gr.cohort && gr.active == 0) gsel = gi;
+    }
+    *group = gsel;
+    if (gsel < 0) return -1;
+    const ServeGroup& gr = groups[gsel];
+    const bool low = kind == CGP_KIND_SSSP;
+    for (int k = 0; k < gr.S; ++k) {
+      const int i = low ? k : gr.S - 1 - k;
+      if (slot_ticket[gr.base + i] < 0) return gr.base + i;
+    }
+    *group = -1;
+    return -1;
+  }
   int best = -1, best_g = -1;
   long long best_key = -1;
   for (int gi = 0; gi < static_cast<int>(groups.size()); ++gi) {
@@ -527,7 +555,7 @@ void cgp_server::loop() {
             continue;
           }
           int gi = -1;
-          const int s = pick_slot(&gi);
+          const int s = pick_slot(&gi, r.q.kind);
           if (s < 0) break;
           ServeGroup& gr = groups[gi];
           pending.pop_front();
