@@ -2292,6 +2292,13 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
     }
     for (int i = threadIdx.x; i < nv * R; i += blockDim.x) s_best[i] = 0xffffffffu;
     __syncthreads();
+    // the rows the commit reads: the 2W lines of 128 bytes of each vertex's
+    // slice move to L2 while the chunk gathers
+    {
+      const int k = static_cast<int>(threadIdx.x >> 3), ln = static_cast<int>(threadIdx.x & 7);
+      if (k < nv && ln < 2 * W && s0 + ln * 32 < g.Qg)
+        prefetch_l2(g.values + static_cast<size_t>(s_v[k]) * Qg + s0 + ln * 32);
+    }
     const int total = s_pre[nv];
     const int seg = (total + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const int fa = min(total, wib * seg);
