@@ -101,10 +101,12 @@ __device__ __forceinline__ void warp_add(unsigned long long x, unsigned long lon
 
 template <int W>
 __device__ __forceinline__ void warp_or_reduce(uint64_t (&m)[W]) {
+  // two redux.sync per word (32-bit halves) instead of a 5-step shuffle tree
 #pragma unroll
   for (int i = 0; i < W; ++i) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m[i] |= __shfl_xor_sync(kFull, m[i], o);
+    const unsigned lo = __reduce_or_sync(kFull, static_cast<unsigned>(m[i]));
+    const unsigned hi = __reduce_or_sync(kFull, static_cast<unsigned>(m[i] >> 32));
+    m[i] = (static_cast<uint64_t>(hi) << 32) | lo;
   }
 }
 
