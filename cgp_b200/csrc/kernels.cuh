@@ -2357,6 +2357,19 @@ __global__ void __launch_bounds__(kBlock, 3) k_sssp_pull_chunked(GroupDev g, Dev
           cnt = screen_qs;
         }
         if (sl == 0) ++scanned;  // in-edges counted once per group
+        if (cnt > 0 && fb - fa <= 32) {
+          // a warp whose whole share is one batch (chunks of low in-degree
+          // vertices, where the gather waits on latency): the source row's
+          // live 128-byte chunks move to L2 now, so that the staged row loads
+          // below wait on L2 rather than on DRAM (on longer shares the extra
+          // requests slowed the bandwidth-bound dense levels)
+          const uint32_t* rb = g.values + static_cast<size_t>(u) * Qg + s0;
+          uint32_t lines = cm & gch;
+          while (lines) {
+            prefetch_l2(rb + 32 * (__ffs(lines) - 1));
+            lines &= lines - 1;
+          }
+        }
       }
       pairs += static_cast<unsigned long long>(cnt);
       const unsigned lm = __ballot_sync(kFull, cnt > 0);
