@@ -191,3 +191,32 @@ def test_group_cohorts_overlap_staggered_arrivals():
     assert min(i.admit_ms for i in infos2) < info1.finish_ms
     for d, o in zip(descs, outs):
         np.testing.assert_array_equal(o, _expected(g, d))
+
+@pytest.mark.parametrize("policy", ["slots", "group"])
+def test_retire_mixes_device_host_and_discarded_outputs(rmat, policy):
+    """Device outputs (written by the retire kernel itself), host outputs
+    (through staging rows) and discarded results retire in the same passes;
+    every kept result is exact."""
+    import torch
+    g, graph = rmat
+    src = g.pick_sources(120, seed=71)
+    kinds = ["bfs", "sssp", "khop"]
+    descs = [cgp.QueryDescriptor(int(s), kinds[i % 3], 2 + i % 4 if i % 3 == 2 else 0)
+             for i, s in enumerate(src)]
+    outs = []
+    for i in range(len(descs)):
+        if (i // 3) % 3 == 0:  # output kinds cycle independently of query kinds
+            outs.append(torch.zeros(g.num_vertices, dtype=torch.int32, device="cuda"))
+        elif (i // 3) % 3 == 1:
+            outs.append(np.zeros(g.num_vertices, np.uint32))
+        else:
+            outs.append(None)
+    with cgp.Server(graph, slots=64, options=cgp.RunOptions(serve_admission=policy)) as s:
+        tickets = [s.submit(d, o) for d, o in zip(descs, outs)]
+        s.drain(timeout_ms=120000)
+        assert all(s.poll(t).state == "done" for t in tickets)
+    for d, o in zip(descs, outs):
+        if o is None:
+            continue
+        got = o.cpu().numpy().view(np.uint32) if hasattr(o, "cpu") else o
+        np.testing.assert_array_equal(got, _expected(g, d))
