@@ -135,6 +135,9 @@ struct DevGraph {
   int64_t heavy_chunks;
   const int32_t* pheavy;            // same for the pull CSR
   const int64_t* pheavy_chunk_start;
+  const int32_t* pheavy_ch;         // per 2048-edge chunk: table index of its vertex
+  const int64_t* pheavy_cb;         // per chunk: first in-edge
+  const int64_t* pheavy_ce;         // per chunk: one past its last in-edge
   int32_t n_pheavy;
   int64_t pheavy_chunks;
   int64_t heavy_degree;

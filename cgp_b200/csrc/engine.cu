@@ -148,6 +148,9 @@ DevGraph GraphImpl::dev_graph(int64_t h) {
   d.heavy_chunks = hp.heavy.chunks;
   d.pheavy = hp.pheavy.vertices.as<int32_t>();
   d.pheavy_chunk_start = hp.pheavy.chunk_start.as<int64_t>();
+  d.pheavy_ch = hp.pheavy.chunk_h.as<int32_t>();
+  d.pheavy_cb = hp.pheavy.chunk_beg.as<int64_t>();
+  d.pheavy_ce = hp.pheavy.chunk_end.as<int64_t>();
   d.n_pheavy = hp.pheavy.n;
   d.pheavy_chunks = hp.pheavy.chunks;
   d.plight = hp.plight.vertices.as<int32_t>();
@@ -181,11 +184,33 @@ void build_heavy(const std::vector<int64_t>& row, int64_t V, int64_t h, HeavyTab
   }
   t.n = static_cast<int32_t>(vs.size());
   t.chunks = cs.back();
+  // per chunk: its vertex's table index and its edge range, so that a CTA
+  // finds its work with three independent loads instead of a binary search
+  std::vector<int32_t> ch(static_cast<size_t>(t.chunks));
+  std::vector<int64_t> cb(static_cast<size_t>(t.chunks)), ce(static_cast<size_t>(t.chunks));
+  for (size_t i = 0; i < vs.size(); ++i) {
+    const int64_t b = row[vs[i]], e = row[vs[i] + 1];
+    for (int64_t c = cs[i]; c < cs[i + 1]; ++c) {
+      ch[c] = static_cast<int32_t>(i);
+      cb[c] = b + (c - cs[i]) * kHeavyChunk;
+      ce[c] = std::min(e, cb[c] + kHeavyChunk);
+    }
+  }
   t.vertices.ensure(std::max<size_t>(vs.size(), 1) * sizeof(int32_t));
   t.chunk_start.ensure(cs.size() * sizeof(int64_t));
-  if (!vs.empty())
+  t.chunk_h.ensure(std::max<size_t>(ch.size(), 1) * sizeof(int32_t));
+  t.chunk_beg.ensure(std::max<size_t>(cb.size(), 1) * sizeof(int64_t));
+  t.chunk_end.ensure(std::max<size_t>(ce.size(), 1) * sizeof(int64_t));
+  if (!vs.empty()) {
     ck(cudaMemcpy(t.vertices.p, vs.data(), vs.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
        "upload heavy");
+    ck(cudaMemcpy(t.chunk_h.p, ch.data(), ch.size() * sizeof(int32_t), cudaMemcpyHostToDevice),
+       "upload heavy chunk vertices");
+    ck(cudaMemcpy(t.chunk_beg.p, cb.data(), cb.size() * sizeof(int64_t), cudaMemcpyHostToDevice),
+       "upload heavy chunk starts");
+    ck(cudaMemcpy(t.chunk_end.p, ce.data(), ce.size() * sizeof(int64_t), cudaMemcpyHostToDevice),
+       "upload heavy chunk ends");
+  }
   ck(cudaMemcpy(t.chunk_start.p, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice),
      "upload heavy chunks");
 }

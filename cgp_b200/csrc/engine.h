@@ -45,6 +45,9 @@ struct DevBuf {
 struct HeavyTable {
   DevBuf vertices;     // int32 [n]
   DevBuf chunk_start;  // int64 [n + 1]
+  DevBuf chunk_h;      // int32 [chunks] table index of each chunk's vertex
+  DevBuf chunk_beg;    // int64 [chunks] first edge of each chunk
+  DevBuf chunk_end;    // int64 [chunks] one past its last edge
   int32_t n = 0;
   int64_t chunks = 0;
 };

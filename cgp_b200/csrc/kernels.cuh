@@ -1007,23 +1007,13 @@ __global__ void __launch_bounds__(kBlock) k_bfs_pull_heavy(GroupDev g, DevGraph 
   const LevelCtl* ctl = g.ctl;
   if (ctl->done || ctl->dir != kDirPull || G.n_pheavy == 0) return;
   const LevelView lv = level_view(g);
-  __shared__ int32_t s_h;
   __shared__ int s_skip;
   __shared__ uint64_t s_red[kWarpsPerBlock][W];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   for (int64_t c = blockIdx.x; c < G.pheavy_chunks; c += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = G.n_pheavy - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (G.pheavy_chunk_start[mid] <= c) lo = mid;
-        else hi = mid - 1;
-      }
-      s_h = lo;
-    }
-    __syncthreads();
-    const int h = s_h;
+    __syncthreads();  // the previous chunk's s_skip is read
+    const int h = G.pheavy_ch[c];
     const int32_t v = G.pheavy[h];
     uint64_t vis[W], need[W];
     load_mask<W>(g.visited + static_cast<size_t>(v) * W, vis);
@@ -1042,10 +1032,8 @@ __global__ void __launch_bounds__(kBlock) k_bfs_pull_heavy(GroupDev g, DevGraph 
     }
     __syncthreads();
     if (s_skip) continue;
-    const int64_t beg = row_at<OT>(G.prow, v);
-    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
-    const int64_t cb = beg + (c - G.pheavy_chunk_start[h]) * kHeavyChunk;
-    const int64_t ce = min(end, cb + kHeavyChunk);
+    const int64_t cb = G.pheavy_cb[c];
+    const int64_t ce = G.pheavy_ce[c];
     uint64_t a[W];
 #pragma unroll
     for (int i = 0; i < W; ++i) a[i] = 0;
@@ -1738,7 +1726,6 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy(GroupDev g, DevGraph
   const LevelView lv = level_view(g);
   constexpr int C = 2 * W;
   __shared__ uint32_t s_best[C * 32];
-  __shared__ int32_t s_h;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const uint64_t* sb = ctl->gsel;
@@ -1749,25 +1736,16 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy(GroupDev g, DevGraph
   for (int i = 0; i < W; ++i) uni[i] = 0;
   unsigned long long improved = 0, pairs = 0;
   unsigned scanned = 0;
+  // every heavy vertex is gathered once per launch (all its chunks)
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    atomicAdd(&g.ctl->lc.spull_vertices, static_cast<unsigned long long>(G.n_pheavy));
   for (int64_t ch = blockIdx.x; ch < G.pheavy_chunks; ch += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = G.n_pheavy - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (G.pheavy_chunk_start[mid] <= ch) lo = mid;
-        else hi = mid - 1;
-      }
-      s_h = lo;
-    }
+    // the chunk's vertex and edge range: independent loads, no search
+    const int32_t v = G.pheavy[G.pheavy_ch[ch]];
+    const int64_t cb = G.pheavy_cb[ch];
+    const int64_t ce = G.pheavy_ce[ch];
     for (int i = threadIdx.x; i < C * 32; i += blockDim.x) s_best[i] = 0xffffffffu;
     __syncthreads();
-    const int h = s_h;
-    const int32_t v = G.pheavy[h];
-    const int64_t beg = row_at<OT>(G.prow, v);
-    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
-    const int64_t cb = beg + (ch - G.pheavy_chunk_start[h]) * kHeavyChunk;
-    const int64_t ce = min(end, cb + kHeavyChunk);
-    if (threadIdx.x == 0 && ch == G.pheavy_chunk_start[h]) atomicAdd(&g.ctl->lc.spull_vertices, 1ULL);
     const int64_t seg = (ce - cb + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const int64_t wb = cb + wib * seg;
     const int64_t we = min(ce, wb + seg);
@@ -2495,7 +2473,6 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   const LevelView lv = level_view(g);
   __shared__ uint32_t s_best[C * 32];
   __shared__ int4 s_stage[kWarpsPerBlock][32];
-  __shared__ int32_t s_h;
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const uint64_t* sb = ctl->gsel;
@@ -2511,25 +2488,16 @@ __global__ void __launch_bounds__(kBlock) k_sssp_pull_heavy_vec(GroupDev g, DevG
   for (int i = 0; i < W; ++i) uni[i] = 0;
   unsigned long long improved = 0, pairs = 0;
   unsigned scanned = 0;
+  // every heavy vertex is gathered once per launch (all its chunks)
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    atomicAdd(&g.ctl->lc.spull_vertices, static_cast<unsigned long long>(G.n_pheavy));
   for (int64_t ch = blockIdx.x; ch < G.pheavy_chunks; ch += gridDim.x) {
-    if (threadIdx.x == 0) {
-      int lo = 0, hi = G.n_pheavy - 1;
-      while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (G.pheavy_chunk_start[mid] <= ch) lo = mid;
-        else hi = mid - 1;
-      }
-      s_h = lo;
-    }
+    // the chunk's vertex and edge range: independent loads, no search
+    const int32_t v = G.pheavy[G.pheavy_ch[ch]];
+    const int64_t cb = G.pheavy_cb[ch];
+    const int64_t ce = G.pheavy_ce[ch];
     for (int i = threadIdx.x; i < C * 32; i += blockDim.x) s_best[i] = 0xffffffffu;
     __syncthreads();
-    const int h = s_h;
-    const int32_t v = G.pheavy[h];
-    const int64_t beg = row_at<OT>(G.prow, v);
-    const int64_t end = row_at<OT>(G.prow, static_cast<int64_t>(v) + 1);
-    const int64_t cb = beg + (ch - G.pheavy_chunk_start[h]) * kHeavyChunk;
-    const int64_t ce = min(end, cb + kHeavyChunk);
-    if (threadIdx.x == 0 && ch == G.pheavy_chunk_start[h]) atomicAdd(&g.ctl->lc.spull_vertices, 1ULL);
     const int64_t seg = (ce - cb + kWarpsPerBlock - 1) / kWarpsPerBlock;
     const int64_t wb = cb + wib * seg;
     const int64_t we = min(ce, wb + seg);
